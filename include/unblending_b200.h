@@ -1,0 +1,95 @@
+/* Extensions of the unblending C ABI in the B200 implementation.
+ *
+ * New symbols only; the v1 entry points of unblending.h are unchanged. They
+ * expose what the v1 signatures cannot carry: the arithmetic precision of
+ * the per-pixel solve, the guided-filter radius (v1 derives it from the
+ * image size, unblending.cpp:351), per-pixel status and work counters,
+ * device-side timings, and device-resident inputs/outputs. None of them has
+ * a counterpart in the reference's C ABI; their semantics follow the
+ * reference functions named beside each. */
+#ifndef UNBLENDING_B200_H
+#define UNBLENDING_B200_H
+
+#include "unblending.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    /* FP32 solve; every pixel's result is re-checked in FP64 and pixels that
+     * miss the feasibility tolerance are re-solved in FP64. */
+    UNBLENDING_PRECISION_FP32 = 0,
+    /* FP64 solve throughout (the reference's FP64 arithmetic). */
+    UNBLENDING_PRECISION_FP64 = 1
+};
+
+/* Controls of the per-pixel augmented-Lagrangian solve
+ * (augmented_lagrangian.cuh:163-167) and of the refinement filter
+ * (unblending.cpp:351-353). */
+typedef struct unblending_solver_options {
+    uint32_t struct_size;
+    int32_t precision;          /* UNBLENDING_PRECISION_*, default FP32 */
+    int32_t starts;             /* 1..3 solver starts, default 1 */
+    int32_t radius;             /* refinement radius; < 0 selects 60 * min(w, h) / 1000 */
+    double epsilon;             /* guided-filter regularizer, default 1e-4 */
+    int32_t resolve_misses;     /* FP32 precision: FP64 re-solve of misses, default 1 */
+    int32_t inner, outer;       /* iteration caps, default 256 and 22 */
+    double inner_tolerance;     /* default 5e-3 */
+    double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
+    int32_t threads_per_block;  /* 0 selects the tuned default */
+} unblending_solver_options;
+
+#define UNBLENDING_SOLVER_OPTIONS_INIT \
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0 }
+
+/* Per-call report. Times are device time measured with CUDA events. */
+typedef struct unblending_stats {
+    uint32_t struct_size;
+    int32_t radius;             /* refinement radius used */
+    int64_t pixels;
+    int64_t misses;             /* pixels whose first solve missed the tolerance */
+    int64_t failed;             /* pixels still missing it at the end */
+    int64_t normalization_failed; /* refinement: pixels whose targets could not be normalized */
+    double ms_upload, ms_filter, ms_solve, ms_resolve, ms_download, ms_total;
+} unblending_stats;
+
+/* unblending_unmix / unblending_refine with solver options, an optional
+ * per-pixel status (n int32: 0 ok, 3 misses the tolerance, 8 refinement
+ * targets not normalizable), optional work counters (n x 5 uint32: values,
+ * gradients, inner iterations, line-search trials, outer steps) and stats.
+ * Any of solver, status, counters, stats may be NULL. */
+UNBLENDING_API int32_t unblending_unmix_ex(
+    const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+    const unblending_options* options, const unblending_solver_options* solver,
+    double* output, size_t output_capacity, int32_t* status, uint32_t* counters, unblending_stats* stats);
+
+UNBLENDING_API int32_t unblending_refine_ex(
+    const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+    const double* first_pass, size_t first_pass_size, const unblending_options* options,
+    const unblending_solver_options* solver, double* output, size_t output_capacity,
+    int32_t* status, uint32_t* counters, unblending_stats* stats);
+
+/* Device-resident variants. All pointers are device memory of the current
+ * CUDA device: image is w*h packed RGB doubles, first_pass/output are packed
+ * [layer][row][column][RGBA] doubles (output may alias first_pass), status
+ * and counters as above (may be NULL). Work is enqueued on `stream` (a
+ * cudaStream_t, NULL selects the library's stream); the call returns without
+ * synchronizing unless `stats` is non-NULL. */
+UNBLENDING_API int32_t unblending_unmix_device(
+    int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
+    const unblending_options* options, const unblending_solver_options* solver,
+    double* output, int32_t* status, uint32_t* counters, void* stream, unblending_stats* stats);
+
+UNBLENDING_API int32_t unblending_refine_device(
+    int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
+    const double* first_pass, const unblending_options* options, const unblending_solver_options* solver,
+    double* output, int32_t* status, uint32_t* counters, void* stream, unblending_stats* stats);
+
+/* Number of GPU kernel launches the most recent call on this thread issued. */
+UNBLENDING_API int64_t unblending_last_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

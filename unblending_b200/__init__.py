@@ -1,0 +1,235 @@
+"""B200-native unblending: colour unmixing and matte refinement on sm_100a.
+
+Python front end of the in-tree C-ABI library `libunblending.so.1` (see
+include/unblending.h and include/unblending_b200.h). The functions mirror the
+reference's buffer API (unblending/include/unblending/pixels.hpp:34-44):
+
+  compute_color_unmixing(image, layers, has_opaque_background)  -> (L, h, w, 4)
+  perform_matte_refinement(image, first, layers, has_opaque_background,
+                           force_smooth_background)             -> (L, h, w, 4)
+
+with the same argument meaning and the same errors (ValueError for
+UNBLENDING_INVALID_ARGUMENT / BUFFER_TOO_SMALL, MemoryError for
+OUT_OF_MEMORY, ExecutionError for CUDA_ERROR / SOLVER_ERROR). There is no CPU
+path: importing this package fails loudly if the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .synthetic import LayerSpec, UnblendingLayer, layer_array  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libunblending.so.1")
+
+OK, INVALID_ARGUMENT, BUFFER_TOO_SMALL, CUDA_ERROR, OUT_OF_MEMORY, SOLVER_ERROR = range(6)
+BACKEND_AUTO, BACKEND_CPU, BACKEND_CUDA = range(3)
+PRECISION_FP32, PRECISION_FP64 = 0, 1
+
+EXPORTED = [
+    "unblending_abi_version", "unblending_unmix", "unblending_refine", "unblending_unmix_ex",
+    "unblending_refine_ex", "unblending_unmix_device", "unblending_refine_device", "unblending_last_launch_count",
+]
+
+
+class ExecutionError(RuntimeError):
+    """A CUDA or solver failure reported by the library (codes 3 and 5)."""
+
+
+class RgbView(ctypes.Structure):
+    _fields_ = [("data", ctypes.POINTER(ctypes.c_double)), ("size", ctypes.c_size_t), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32), ("row_stride", ctypes.c_size_t)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("backend", ctypes.c_int32), ("opaque_background", ctypes.c_int32),
+                ("smooth_background", ctypes.c_int32), ("target_concurrency", ctypes.c_int32)]
+
+
+class SolverOptions(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("precision", ctypes.c_int32), ("starts", ctypes.c_int32),
+                ("radius", ctypes.c_int32), ("epsilon", ctypes.c_double), ("resolve_misses", ctypes.c_int32),
+                ("inner", ctypes.c_int32), ("outer", ctypes.c_int32), ("inner_tolerance", ctypes.c_double),
+                ("outer_tolerance", ctypes.c_double), ("threads_per_block", ctypes.c_int32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("radius", ctypes.c_int32), ("pixels", ctypes.c_int64),
+                ("misses", ctypes.c_int64), ("failed", ctypes.c_int64), ("normalization_failed", ctypes.c_int64),
+                ("ms_upload", ctypes.c_double), ("ms_filter", ctypes.c_double), ("ms_solve", ctypes.c_double),
+                ("ms_resolve", ctypes.c_double), ("ms_download", ctypes.c_double), ("ms_total", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "struct_size"}
+
+
+def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> Options:
+    return Options(ctypes.sizeof(Options), backend, int(opaque), int(smooth), concurrency)
+
+
+def solver_options(precision=PRECISION_FP32, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
+                   outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0) -> SolverOptions:
+    return SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
+                         outer, inner_tolerance, outer_tolerance, threads_per_block)
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m unblending_b200.build` (or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, dp = ctypes.POINTER, ctypes.POINTER(ctypes.c_double)
+    lib.unblending_abi_version.restype = ctypes.c_uint32
+    lib.unblending_unmix.restype = ctypes.c_int32
+    lib.unblending_unmix.argtypes = [P(RgbView), ctypes.c_void_p, ctypes.c_size_t, P(Options), dp, ctypes.c_size_t]
+    lib.unblending_refine.restype = ctypes.c_int32
+    lib.unblending_refine.argtypes = [P(RgbView), ctypes.c_void_p, ctypes.c_size_t, dp, ctypes.c_size_t, P(Options),
+                                      dp, ctypes.c_size_t]
+    lib.unblending_unmix_ex.restype = ctypes.c_int32
+    lib.unblending_unmix_ex.argtypes = [P(RgbView), ctypes.c_void_p, ctypes.c_size_t, P(Options), P(SolverOptions),
+                                        dp, ctypes.c_size_t, P(ctypes.c_int32), P(ctypes.c_uint32), P(Stats)]
+    lib.unblending_refine_ex.restype = ctypes.c_int32
+    lib.unblending_refine_ex.argtypes = [P(RgbView), ctypes.c_void_p, ctypes.c_size_t, dp, ctypes.c_size_t,
+                                         P(Options), P(SolverOptions), dp, ctypes.c_size_t, P(ctypes.c_int32),
+                                         P(ctypes.c_uint32), P(Stats)]
+    lib.unblending_unmix_device.restype = ctypes.c_int32
+    lib.unblending_unmix_device.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, P(Stats)]
+    lib.unblending_refine_device.restype = ctypes.c_int32
+    lib.unblending_refine_device.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_size_t, ctypes.c_void_p, P(Options), P(SolverOptions),
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             P(Stats)]
+    lib.unblending_last_launch_count.restype = ctypes.c_int64
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc: int):
+    if rc == OK:
+        return
+    if rc in (INVALID_ARGUMENT, BUFFER_TOO_SMALL):
+        raise ValueError(f"unblending rejected its arguments (code {rc})")
+    if rc == OUT_OF_MEMORY:
+        raise MemoryError("unblending: out of device memory")
+    raise ExecutionError(f"unblending failed (code {rc})")
+
+
+def _layers(layers):
+    if isinstance(layers, ctypes.Array):
+        return layers, len(layers)
+    arr = layer_array(list(layers))
+    return arr, len(arr)
+
+
+def _view(image: np.ndarray) -> tuple[RgbView, np.ndarray]:
+    img = np.asarray(image, dtype=np.float64)
+    if img.ndim != 3 or img.shape[2] != 3:
+        raise ValueError("image must be (height, width, 3)")
+    if not img.flags.c_contiguous:
+        img = np.ascontiguousarray(img)
+    h, w, _ = img.shape
+    return RgbView(img.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), img.size, w, h, 0), img
+
+
+def unmix_ex(image, layers, opaque=True, solver=None, backend=BACKEND_AUTO, with_status=True, with_counters=False):
+    """First pass. Returns (packed (L,h,w,4), status (n,) | None, counters (n,5) | None, stats dict)."""
+    view, keep = _view(image)
+    arr, L = _layers(layers)
+    h, w = keep.shape[:2]
+    out = np.empty((L, h, w, 4))
+    status = np.empty(h * w, np.int32) if with_status else None
+    counters = np.empty((h * w, 5), np.uint32) if with_counters else None
+    stats = Stats(); stats.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_unmix_ex(ctypes.byref(view), arr, L, ctypes.byref(options(opaque, False, backend)),
+                                 ctypes.byref(solver or solver_options()),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size,
+                                 status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if status is not None else None,
+                                 counters.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if counters is not None else None,
+                                 ctypes.byref(stats))
+    _check(rc)
+    return out, status, counters, stats.as_dict()
+
+
+def refine_ex(image, first, layers, opaque=True, smooth=False, solver=None, backend=BACKEND_AUTO, with_status=True,
+              with_counters=False):
+    """Refinement. Returns (packed (L,h,w,4), status, counters, stats dict)."""
+    view, keep = _view(image)
+    arr, L = _layers(layers)
+    h, w = keep.shape[:2]
+    first = np.ascontiguousarray(first, dtype=np.float64)
+    out = np.empty((L, h, w, 4))
+    status = np.empty(h * w, np.int32) if with_status else None
+    counters = np.empty((h * w, 5), np.uint32) if with_counters else None
+    stats = Stats(); stats.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_refine_ex(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  first.size, ctypes.byref(options(opaque, smooth, backend)),
+                                  ctypes.byref(solver or solver_options()),
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size,
+                                  status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if status is not None else None,
+                                  counters.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if counters is not None else None,
+                                  ctypes.byref(stats))
+    _check(rc)
+    return out, status, counters, stats.as_dict()
+
+
+def compute_color_unmixing(image, layer_infos, has_opaque_background=True, target_concurrency=0):
+    """Reference buffer API (pixels.hpp:34-37): packed (L, h, w, 4) RGBA doubles."""
+    view, keep = _view(image)
+    arr, L = _layers(layer_infos)
+    h, w = keep.shape[:2]
+    out = np.empty((L, h, w, 4))
+    rc = lib.unblending_unmix(ctypes.byref(view), arr, L,
+                              ctypes.byref(options(has_opaque_background, False, BACKEND_AUTO, target_concurrency)),
+                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
+    _check(rc)
+    return out
+
+
+def perform_matte_refinement(image, layers, layer_infos, has_opaque_background=True, force_smooth_background=False,
+                             target_concurrency=0):
+    """Reference buffer API (pixels.hpp:40-44): packed (L, h, w, 4) RGBA doubles."""
+    view, keep = _view(image)
+    arr, L = _layers(layer_infos)
+    h, w = keep.shape[:2]
+    first = np.ascontiguousarray(layers, dtype=np.float64)
+    out = np.empty((L, h, w, 4))
+    rc = lib.unblending_refine(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               first.size, ctypes.byref(options(has_opaque_background, force_smooth_background,
+                                                                BACKEND_AUTO, target_concurrency)),
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
+    _check(rc)
+    return out
+
+
+def unmix_device(width, height, d_image, layers, d_output, opaque=True, solver=None, d_status=None, d_counters=None,
+                 stream=None, stats=False):
+    """Device-resident first pass on raw device pointers (ints). Returns stats dict or None."""
+    arr, L = _layers(layers)
+    st = Stats(); st.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_unmix_device(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+                                     ctypes.byref(solver or solver_options()), d_output, d_status, d_counters, stream,
+                                     ctypes.byref(st) if stats else None)
+    _check(rc)
+    return st.as_dict() if stats else None
+
+
+def refine_device(width, height, d_image, layers, d_first, d_output, opaque=True, smooth=False, solver=None,
+                  d_status=None, d_counters=None, stream=None, stats=False):
+    """Device-resident refinement on raw device pointers (ints). Returns stats dict or None."""
+    arr, L = _layers(layers)
+    st = Stats(); st.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_refine_device(width, height, d_image, arr, L, d_first, ctypes.byref(options(opaque, smooth)),
+                                      ctypes.byref(solver or solver_options()), d_output, d_status, d_counters, stream,
+                                      ctypes.byref(st) if stats else None)
+    _check(rc)
+    return st.as_dict() if stats else None
+
+
+def last_launch_count() -> int:
+    return int(lib.unblending_last_launch_count())

@@ -1,0 +1,478 @@
+// C ABI of the B200 unblending path: validation, device context, and the
+// orchestration of upload -> (filter) -> solve -> FP64 check/re-solve ->
+// download on one CUDA stream.
+//
+// Mirrors the reference's C layer (sdk/unblending_c.cpp:23-110) and the
+// argument checks of its buffer API (unblending.cpp:505-534,590-604):
+// same validation order, same error codes, output written only on success.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <vector>
+
+#include "../../include/unblending.h"
+#include "../../include/unblending_b200.h"
+#include "solver_dispatch.hpp"
+
+namespace {
+
+using namespace unb;
+
+struct CudaFailure : std::runtime_error {
+    cudaError_t code;
+    explicit CudaFailure(cudaError_t c) : std::runtime_error(cudaGetErrorString(c)), code(c) {}
+};
+struct SolverFailure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); throw std::bad_alloc(); }
+    throw CudaFailure(e);
+}
+
+thread_local int64_t t_launches = 0;
+
+// Grow-only device allocation.
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    template <class T> T* get(size_t count) {
+        const size_t want = std::max<size_t>(count * sizeof(T), 256);
+        if (want > bytes) {
+            if (ptr) cudaFree(ptr);
+            ptr = nullptr; bytes = 0;
+            ck(cudaMalloc(&ptr, want));
+            bytes = want;
+        }
+        return static_cast<T*>(ptr);
+    }
+};
+
+// One per CUDA device: a stream, the solver's scratch, and timing events.
+// Calls on the same device are serialized by `mutex`.
+struct Context {
+    int device = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    std::mutex mutex;
+    Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters;
+    explicit Context(int dev) : device(dev) {
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        for (auto& e : ev) ck(cudaEventCreate(&e));
+    }
+};
+
+Context& context() {
+    static std::mutex registry_mutex;
+    static std::map<int, std::unique_ptr<Context>> registry;
+    int dev = 0;
+    ck(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(registry_mutex);
+    auto& slot = registry[dev];
+    if (!slot) slot = std::make_unique<Context>(dev);
+    return *slot;
+}
+
+// ------------------------------------------------------------- validation --
+struct Spec {
+    int width = 0, height = 0, layers = 0;
+    size_t pixels = 0, required = 0, row_stride = 0;
+    bool opaque = true, smooth = false, strict = false, plus = false, source_over = true;
+};
+
+bool symmetric_pd(const double* p) {
+    // Symmetric within 1e-12 relative (Frobenius), then a Cholesky pivot test
+    // (sdk/unblending_c.cpp:39-41: isApprox(transpose, 1e-12) and LLT success).
+    double diff = 0, norm = 0;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            const double d = p[3 * r + c] - p[3 * c + r];
+            diff += d * d;
+            norm += p[3 * r + c] * p[3 * r + c];
+        }
+    if (!(diff <= 1e-24 * norm)) return false;
+    const double l00 = p[0];
+    if (!(l00 > 0)) return false;
+    const double a = std::sqrt(l00), l10 = p[3] / a, l20 = p[6] / a;
+    const double d1 = p[4] - l10 * l10;
+    if (!(d1 > 0)) return false;
+    const double b = std::sqrt(d1), l21 = (p[7] - l20 * l10) / b;
+    const double d2 = p[8] - l20 * l20 - l21 * l21;
+    return d2 > 0;
+}
+
+int32_t validate(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                 const unblending_options* options, const double* output, size_t output_capacity, bool refine,
+                 const double* first, size_t first_size, Spec& s, bool device_mode) {
+    constexpr int max_int = std::numeric_limits<int>::max();
+    if (!image || !layers || !layer_count || layer_count > size_t(max_int) / 4 || image->width <= 0 ||
+        image->height <= 0 || image->width > max_int / image->height)
+        return UNBLENDING_INVALID_ARGUMENT;
+    const size_t pixels = size_t(image->width) * size_t(image->height);
+    if (pixels > (std::numeric_limits<size_t>::max() / sizeof(double)) / 4 / layer_count)
+        return UNBLENDING_INVALID_ARGUMENT;
+    const size_t required = 4 * pixels * layer_count;
+    if (!device_mode && output_capacity < required) return UNBLENDING_BUFFER_TOO_SMALL;
+    if (!output) return UNBLENDING_INVALID_ARGUMENT;
+
+    const unblending_options defaults = UNBLENDING_OPTIONS_INIT;
+    if (!options) options = &defaults;
+    if (options->struct_size < sizeof(unblending_options) ||
+        (options->opaque_background != 0 && options->opaque_background != 1) ||
+        (options->smooth_background != 0 && options->smooth_background != 1) || options->target_concurrency < 0)
+        return UNBLENDING_INVALID_ARGUMENT;
+    if (options->backend != UNBLENDING_BACKEND_AUTO && options->backend != UNBLENDING_BACKEND_CUDA)
+        return UNBLENDING_INVALID_ARGUMENT;   // unknown backend, or CPU: no CPU path in this library
+
+    for (size_t l = 0; l < layer_count; ++l) {
+        const auto& L = layers[l];
+        if (L.blend_mode < UNBLENDING_NORMAL || L.blend_mode > UNBLENDING_LINEAR_DODGE) return UNBLENDING_INVALID_ARGUMENT;
+        for (double v : L.mean) if (!std::isfinite(v)) return UNBLENDING_INVALID_ARGUMENT;
+        for (double v : L.precision) if (!std::isfinite(v)) return UNBLENDING_INVALID_ARGUMENT;
+        if (!symmetric_pd(L.precision)) return UNBLENDING_INVALID_ARGUMENT;
+    }
+
+    // Buffer API checks (unblending.cpp:508-534).
+    if (!image->data) return UNBLENDING_INVALID_ARGUMENT;
+    const size_t row_size = 3 * size_t(image->width);
+    size_t stride = image->row_stride ? image->row_stride : row_size;
+    if (!device_mode) {
+        if (stride < row_size || image->size < row_size ||
+            size_t(image->height - 1) > (image->size - row_size) / stride)
+            return UNBLENDING_INVALID_ARGUMENT;
+    } else {
+        stride = row_size;
+    }
+    if (layer_count > size_t(kMaxLayers)) return UNBLENDING_INVALID_ARGUMENT;   // compiled layer counts
+    if (pixels > size_t(max_int)) return UNBLENDING_INVALID_ARGUMENT;
+
+    s.width = image->width; s.height = image->height; s.layers = int(layer_count);
+    s.pixels = pixels; s.required = required; s.row_stride = stride;
+    s.opaque = options->opaque_background != 0;
+    s.smooth = options->smooth_background != 0;
+    s.strict = options->backend == UNBLENDING_BACKEND_CUDA;
+    s.plus = true; s.source_over = true;
+    for (size_t l = 0; l < layer_count; ++l) {
+        const auto& L = layers[l];
+        s.plus &= L.comp_x == 2 && L.comp_y == 1 && L.comp_z == 1;
+        s.source_over &= L.comp_x == 1 && L.comp_y == 1 && L.comp_z == 1;
+    }
+    if (refine) {
+        // unblending.cpp:597-604
+        if (!first || (!device_mode && first_size != required)) return UNBLENDING_INVALID_ARGUMENT;
+        if (s.smooth && !s.opaque) return UNBLENDING_INVALID_ARGUMENT;
+        if (!s.plus && !s.source_over) return UNBLENDING_INVALID_ARGUMENT;
+    } else {
+        s.smooth = false;   // smoothing applies to refinement only
+    }
+    return UNBLENDING_OK;
+}
+
+int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_options& out) {
+    const unblending_solver_options defaults = UNBLENDING_SOLVER_OPTIONS_INIT;
+    out = defaults;
+    if (!in) return UNBLENDING_OK;
+    if (in->struct_size < sizeof(unblending_solver_options)) return UNBLENDING_INVALID_ARGUMENT;
+    out = *in;
+    out.struct_size = sizeof(unblending_solver_options);
+    if ((out.precision != UNBLENDING_PRECISION_FP32 && out.precision != UNBLENDING_PRECISION_FP64) ||
+        out.starts < 1 || out.starts > 3 || !(out.epsilon > 0) || !std::isfinite(out.epsilon) || out.inner < 1 ||
+        out.outer < 1 || !(out.inner_tolerance > 0) || !(out.outer_tolerance > 0) ||
+        (out.resolve_misses != 0 && out.resolve_misses != 1) ||
+        (out.threads_per_block != 0 && (out.threads_per_block % 32 != 0 || out.threads_per_block < 32 ||
+                                        out.threads_per_block > 1024)))
+        return UNBLENDING_INVALID_ARGUMENT;
+    return UNBLENDING_OK;
+}
+
+template <class T> Models<T> make_models(const unblending_layer* layers, int L) {
+    Models<T> m{};
+    for (int l = 0; l < L; ++l) {
+        for (int r = 0; r < 3; ++r) m.mean[l][r] = T(layers[l].mean[r]);
+        for (int k = 0; k < 9; ++k) m.prec[l][k] = T(layers[l].precision[k]);
+        m.mode[l] = layers[l].blend_mode;
+        m.X[l] = layers[l].comp_x; m.Y[l] = layers[l].comp_y; m.Z[l] = layers[l].comp_z;
+    }
+    return m;
+}
+
+// --------------------------------------------------------------- a pass --
+struct PassIO {
+    const double* image = nullptr;   // device, packed RGB
+    const double* first = nullptr;   // device, refinement
+    double* out = nullptr;           // device
+    int32_t* status = nullptr;       // device, per pixel (context buffer when the caller passes none)
+    uint32_t* counters = nullptr;    // device or null
+};
+
+struct PassResult {
+    int32_t* small = nullptr;   // device: [0] misses, [1] failures after re-solve, [2] normalization failures
+    int radius = 0;
+};
+
+// Enqueues one pass on `s`. Events ev[0..3] bracket filter / solve / re-solve.
+PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblending_layer* layers,
+                        const unblending_solver_options& so, const PassIO& io, cudaStream_t s) {
+    PassResult R;
+    const int L = sp.layers;
+    const size_t n = sp.pixels;
+    uint32_t* queues = c.small.get<uint32_t>(8);
+    int32_t* counts = reinterpret_cast<int32_t*>(queues + 4);
+    R.small = counts;
+    ck(cudaMemsetAsync(queues, 0, 8 * sizeof(uint32_t), s));
+
+    ck(cudaEventRecord(c.ev[0], s));
+    double* targets = nullptr;
+    int32_t* fstatus = nullptr;
+    if (refine) {
+        R.radius = so.radius >= 0 ? so.radius : 60 * std::min(sp.width, sp.height) / 1000;
+        FilterArgs f;
+        f.width = sp.width; f.height = sp.height; f.layers = L; f.radius = R.radius; f.eps = so.epsilon;
+        f.opaque = sp.opaque; f.smooth = sp.smooth; f.plus = sp.plus;
+        f.image = io.image; f.first = io.first;
+        targets = c.targets.get<double>((size_t(L) + 3) * n);
+        fstatus = c.fstatus.get<int32_t>(n);
+        f.targets = targets; f.status = fstatus;
+        f.scratch = R.radius > 0 ? c.scratch.get<double>(filter_scratch_doubles(sp.width, sp.height, L, sp.smooth)) : nullptr;
+        ck(launch_filter(f, s));
+        t_launches += R.radius > 0 ? 7 : 1;
+    }
+    ck(cudaEventRecord(c.ev[1], s));
+
+    SolverControls ctl;
+    ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
+    ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+    SolveArgs a;
+    a.n = int(n);
+    a.image = io.image; a.first = io.first; a.targets = targets; a.out = io.out;
+    a.status = io.status; a.counters = io.counters;
+    a.input_status = fstatus; a.input_failed = counts + 2;
+    a.opaque = sp.opaque; a.smooth = sp.smooth;
+    a.queue = queues;
+    a.miss_list = c.list_a.get<int32_t>(n);
+    a.miss_count = counts + 0;
+    const int threads = so.threads_per_block ? so.threads_per_block : 128;
+    if (so.precision == UNBLENDING_PRECISION_FP64) {
+        ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, a, threads, c.sms, s));
+        ++t_launches;
+        ck(cudaEventRecord(c.ev[2], s));
+        ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    } else {
+        ck(launch_solve_fp32(L, refine, make_models<float>(layers, L), ctl, a, threads, c.sms, s));
+        ++t_launches;
+        ck(cudaEventRecord(c.ev[2], s));
+        if (so.resolve_misses) {
+            SolveArgs b = a;
+            b.list = a.miss_list; b.list_count = counts + 0;
+            b.miss_list = c.list_b.get<int32_t>(n);
+            b.miss_count = counts + 1;
+            b.queue = queues + 1;
+            b.input_status = nullptr; b.input_failed = nullptr;
+            ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, b, threads, c.sms, s));
+            ++t_launches;
+        } else {
+            ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+        }
+    }
+    ck(cudaEventRecord(c.ev[3], s));
+    return R;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? ms : 0.f;
+}
+
+template <class F> int32_t guarded(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) { return UNBLENDING_OUT_OF_MEMORY; }
+    catch (const CudaFailure& e) { cudaGetLastError(); return UNBLENDING_CUDA_ERROR; }
+    catch (const SolverFailure&) { return UNBLENDING_CUDA_ERROR; }
+    catch (const std::invalid_argument&) { return UNBLENDING_INVALID_ARGUMENT; }
+    catch (const std::length_error&) { return UNBLENDING_INVALID_ARGUMENT; }
+    catch (...) { return UNBLENDING_SOLVER_ERROR; }
+}
+
+// Host-buffer call: upload, pass, check, download.
+int32_t host_call(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                  const double* first, size_t first_size, const unblending_options* options,
+                  const unblending_solver_options* solver, double* output, size_t output_capacity, int32_t* status,
+                  uint32_t* counters, unblending_stats* stats, bool refine) {
+    t_launches = 0;
+    Spec sp;
+    int32_t rc = validate(image, layers, layer_count, options, output, output_capacity, refine, first, first_size, sp,
+                          false);
+    if (rc != UNBLENDING_OK) return rc;
+    unblending_solver_options so;
+    if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
+    if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = c.stream;
+        const size_t n = sp.pixels, L = size_t(sp.layers);
+        PassIO io;
+        double* d_image = c.image.get<double>(3 * n);
+        cudaEvent_t t0, t1;
+        ck(cudaEventCreate(&t0)); ck(cudaEventCreate(&t1));
+        struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{t0, t1};
+        ck(cudaEventRecord(t0, s));
+        const size_t row = 3 * size_t(sp.width);
+        if (sp.row_stride == row)
+            ck(cudaMemcpyAsync(d_image, image->data, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+        else
+            ck(cudaMemcpy2DAsync(d_image, row * sizeof(double), image->data, sp.row_stride * sizeof(double),
+                                 row * sizeof(double), size_t(sp.height), cudaMemcpyHostToDevice, s));
+        io.image = d_image;
+        if (refine) {
+            double* d_first = c.first.get<double>(4 * L * n);
+            ck(cudaMemcpyAsync(d_first, first, 4 * L * n * sizeof(double), cudaMemcpyHostToDevice, s));
+            io.first = d_first;
+        }
+        io.out = c.out.get<double>(4 * L * n);
+        io.status = c.status.get<int32_t>(n);
+        io.counters = counters ? c.counters.get<uint32_t>(5 * n) : nullptr;
+        PassResult R = enqueue_pass(c, sp, refine, layers, so, io, s);
+        int32_t counts[3] = {0, 0, 0};
+        ck(cudaMemcpyAsync(counts, R.small, sizeof(counts), cudaMemcpyDeviceToHost, s));
+        ck(cudaStreamSynchronize(s));
+        if (sp.strict && (counts[1] > 0 || counts[2] > 0)) throw SolverFailure("pixels miss the feasibility tolerance");
+        ck(cudaEventRecord(c.ev[4], s));
+        ck(cudaMemcpyAsync(output, io.out, 4 * L * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (status) ck(cudaMemcpyAsync(status, io.status, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        if (counters) ck(cudaMemcpyAsync(counters, io.counters, 5 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        ck(cudaEventRecord(t1, s));
+        ck(cudaStreamSynchronize(s));
+        ck(cudaGetLastError());
+        if (stats) {
+            stats->radius = R.radius;
+            stats->pixels = int64_t(n);
+            stats->misses = counts[0];
+            stats->failed = counts[1];
+            stats->normalization_failed = counts[2];
+            stats->ms_upload = elapsed(t0, c.ev[0]);
+            stats->ms_filter = elapsed(c.ev[0], c.ev[1]);
+            stats->ms_solve = elapsed(c.ev[1], c.ev[2]);
+            stats->ms_resolve = elapsed(c.ev[2], c.ev[3]);
+            stats->ms_download = elapsed(c.ev[4], t1);
+            stats->ms_total = elapsed(t0, t1);
+        }
+        return UNBLENDING_OK;
+    });
+}
+
+int32_t device_call(int32_t width, int32_t height, const double* image, const unblending_layer* layers,
+                    size_t layer_count, const double* first, const unblending_options* options,
+                    const unblending_solver_options* solver, double* output, int32_t* status, uint32_t* counters,
+                    void* stream, unblending_stats* stats, bool refine) {
+    t_launches = 0;
+    unblending_rgb_view view{image, 0, width, height, 0};
+    Spec sp;
+    int32_t rc = validate(&view, layers, layer_count, options, output, 0, refine, first, 0, sp, true);
+    if (rc != UNBLENDING_OK) return rc;
+    unblending_solver_options so;
+    if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
+    if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+        PassIO io;
+        io.image = image; io.first = first; io.out = output;
+        if (refine && first == output && so.precision == UNBLENDING_PRECISION_FP32 && so.resolve_misses) {
+            // The FP64 re-solve reads the first pass of pixels the FP32 solve
+            // has already overwritten: keep a private copy.
+            double* copy = c.first.get<double>(4 * size_t(sp.layers) * sp.pixels);
+            ck(cudaMemcpyAsync(copy, first, 4 * size_t(sp.layers) * sp.pixels * sizeof(double),
+                               cudaMemcpyDeviceToDevice, s));
+            io.first = copy;
+        }
+        io.status = status ? status : c.status.get<int32_t>(sp.pixels);
+        io.counters = counters;
+        PassResult R = enqueue_pass(c, sp, refine, layers, so, io, s);
+        if (stats) {
+            int32_t counts[3] = {0, 0, 0};
+            ck(cudaMemcpyAsync(counts, R.small, sizeof(counts), cudaMemcpyDeviceToHost, s));
+            ck(cudaStreamSynchronize(s));
+            stats->radius = R.radius;
+            stats->pixels = int64_t(sp.pixels);
+            stats->misses = counts[0];
+            stats->failed = counts[1];
+            stats->normalization_failed = counts[2];
+            stats->ms_upload = 0;
+            stats->ms_filter = elapsed(c.ev[0], c.ev[1]);
+            stats->ms_solve = elapsed(c.ev[1], c.ev[2]);
+            stats->ms_resolve = elapsed(c.ev[2], c.ev[3]);
+            stats->ms_download = 0;
+            stats->ms_total = elapsed(c.ev[0], c.ev[3]);
+            if (sp.strict && (counts[1] > 0 || counts[2] > 0)) throw SolverFailure("pixels miss the feasibility tolerance");
+        }
+        ck(cudaPeekAtLastError());
+        return UNBLENDING_OK;
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t unblending_abi_version(void) { return UNBLENDING_ABI_VERSION; }
+
+int32_t unblending_unmix(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                         const unblending_options* options, double* output, size_t output_capacity) {
+    return host_call(image, layers, layer_count, nullptr, 0, options, nullptr, output, output_capacity, nullptr,
+                     nullptr, nullptr, false);
+}
+
+int32_t unblending_refine(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                          const double* first_pass, size_t first_pass_size, const unblending_options* options,
+                          double* output, size_t output_capacity) {
+    return host_call(image, layers, layer_count, first_pass, first_pass_size, options, nullptr, output,
+                     output_capacity, nullptr, nullptr, nullptr, true);
+}
+
+int32_t unblending_unmix_ex(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                            const unblending_options* options, const unblending_solver_options* solver,
+                            double* output, size_t output_capacity, int32_t* status, uint32_t* counters,
+                            unblending_stats* stats) {
+    return host_call(image, layers, layer_count, nullptr, 0, options, solver, output, output_capacity, status,
+                     counters, stats, false);
+}
+
+int32_t unblending_refine_ex(const unblending_rgb_view* image, const unblending_layer* layers, size_t layer_count,
+                             const double* first_pass, size_t first_pass_size, const unblending_options* options,
+                             const unblending_solver_options* solver, double* output, size_t output_capacity,
+                             int32_t* status, uint32_t* counters, unblending_stats* stats) {
+    return host_call(image, layers, layer_count, first_pass, first_pass_size, options, solver, output,
+                     output_capacity, status, counters, stats, true);
+}
+
+int32_t unblending_unmix_device(int32_t width, int32_t height, const double* image, const unblending_layer* layers,
+                                size_t layer_count, const unblending_options* options,
+                                const unblending_solver_options* solver, double* output, int32_t* status,
+                                uint32_t* counters, void* stream, unblending_stats* stats) {
+    return device_call(width, height, image, layers, layer_count, nullptr, options, solver, output, status, counters,
+                       stream, stats, false);
+}
+
+int32_t unblending_refine_device(int32_t width, int32_t height, const double* image, const unblending_layer* layers,
+                                 size_t layer_count, const double* first_pass, const unblending_options* options,
+                                 const unblending_solver_options* solver, double* output, int32_t* status,
+                                 uint32_t* counters, void* stream, unblending_stats* stats) {
+    return device_call(width, height, image, layers, layer_count, first_pass, options, solver, output, status,
+                       counters, stream, stats, true);
+}
+
+int64_t unblending_last_launch_count(void) { return t_launches; }
+
+}  // extern "C"
