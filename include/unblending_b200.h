@@ -38,10 +38,11 @@ typedef struct unblending_solver_options {
     double inner_tolerance;     /* default 5e-3 */
     double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
     int32_t threads_per_block;  /* 0 selects the tuned default */
+    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1 in shared memory */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1 }
 
 /* Per-call report. Times are device time measured with CUDA events. */
 typedef struct unblending_stats {

@@ -1,0 +1,138 @@
+"""The C-ABI library: it loads, exports exactly what include/*.h declares,
+and rejects invalid arguments with the reference's error codes before any
+device work (unblending_c.cpp:57-74, unblending.cpp:508-534,597-604), so
+these tests need no GPU."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import unblending_b200 as U
+from unblending_b200 import synthetic as syn
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("unblending.h", "unblending_b200.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"UNBLENDING_API\s+[\w\s\*]+?\b(unblending_\w+)\s*\(", text))
+    return names
+
+
+def test_every_declared_symbol_is_exported():
+    declared = declared_symbols()
+    assert {"unblending_abi_version", "unblending_unmix", "unblending_refine"} <= declared
+    for name in declared:
+        assert hasattr(U.lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", U.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported_c = {line.split()[-1] for line in out.splitlines() if line.split()[-1].startswith("unblending_")}
+    assert exported_c == declared
+
+
+def test_soname_and_abi_version():
+    out = subprocess.run(["readelf", "-d", U.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    assert "libunblending.so.1" in out
+    assert U.lib.unblending_abi_version() == 1
+
+
+def _call_unmix(image, layers, L=None, opts=None, out=None, capacity=None):
+    view, keep = U._view(image) if image is not None else (None, None)
+    arr = syn.layer_array(layers) if layers is not None else None
+    L = len(layers) if L is None else L
+    if out is None:
+        out = np.empty(4 * 30 * max(L, 1))
+    cap = out.size if capacity is None else capacity
+    return U.lib.unblending_unmix(ctypes.byref(view) if view is not None else None, arr, L,
+                                  ctypes.byref(opts) if opts is not None else None,
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)
+
+
+@pytest.fixture
+def small():
+    return syn.workload("rgb256_l3", 6, 5)
+
+
+def test_invalid_arguments(small):
+    img, layers = small.image, small.layers
+    assert _call_unmix(None, layers) == U.INVALID_ARGUMENT
+    assert _call_unmix(img, layers, L=0) == U.INVALID_ARGUMENT
+    assert _call_unmix(img, layers, capacity=10) == U.BUFFER_TOO_SMALL
+    for bad in [dict(opaque=2), dict(smooth=-1), dict(concurrency=-1)]:
+        o = U.options(**bad)
+        assert _call_unmix(img, layers, opts=o) == U.INVALID_ARGUMENT
+    o = U.options(); o.struct_size = 4
+    assert _call_unmix(img, layers, opts=o) == U.INVALID_ARGUMENT
+    o = U.options(backend=7)
+    assert _call_unmix(img, layers, opts=o) == U.INVALID_ARGUMENT
+    # No CPU path in the library: CPU backend is an invalid argument.
+    assert _call_unmix(img, layers, opts=U.options(backend=U.BACKEND_CPU)) == U.INVALID_ARGUMENT
+
+
+def test_invalid_layers(small):
+    img = small.image
+    for mutate in ("mode", "nan_mean", "asym", "not_pd"):
+        layers = [syn.LayerSpec(l.mode, l.mean.copy(), l.covariance.copy(), l.comp) for l in small.layers]
+        arr = syn.layer_array(layers)
+        if mutate == "mode":
+            arr[1].blend_mode = 13
+        elif mutate == "nan_mean":
+            arr[0].mean[1] = float("nan")
+        elif mutate == "asym":
+            arr[2].precision[1] += 1e-3
+        else:
+            for k, v in enumerate([1, 2, 0, 2, 1, 0, 0, 0, 1]):
+                arr[1].precision[k] = v
+        view, keep = U._view(img)
+        out = np.empty(4 * img.shape[0] * img.shape[1] * 3)
+        rc = U.lib.unblending_unmix(ctypes.byref(view), arr, 3, None,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
+        assert rc == U.INVALID_ARGUMENT, mutate
+
+
+def test_invalid_image_views(small):
+    arr = syn.layer_array(small.layers)
+    img = np.ascontiguousarray(small.image)
+    out = np.empty(4 * 30 * 3)
+    p = img.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    op = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cases = [
+        U.RgbView(p, img.size, 0, 5, 0),             # zero width
+        U.RgbView(p, img.size, 6, -1, 0),            # negative height
+        U.RgbView(p, img.size, 6, 5, 17),            # stride < 3 * width
+        U.RgbView(p, img.size - 1, 6, 5, 0),         # buffer too small for its rows
+        U.RgbView(None, img.size, 6, 5, 0),          # null data
+    ]
+    for v in cases:
+        assert U.lib.unblending_unmix(ctypes.byref(v), arr, 3, None, op, out.size) == U.INVALID_ARGUMENT
+
+
+def test_refine_argument_rules(small):
+    img, layers = small.image, small.layers
+    first = np.zeros((3, 5, 6, 4))
+    with pytest.raises(ValueError):   # smoothing needs an opaque background
+        U.perform_matte_refinement(img, first, layers, has_opaque_background=False, force_smooth_background=True)
+    with pytest.raises(ValueError):   # wrong first-pass size
+        U.perform_matte_refinement(img, first[:2], layers)
+    mixed = [syn.LayerSpec(l.mode, l.mean, l.covariance, syn.PLUS if i == 1 else syn.SOURCE_OVER)
+             for i, l in enumerate(layers)]
+    with pytest.raises(ValueError):   # neither all-Plus nor all-SourceOver
+        U.perform_matte_refinement(img, first, mixed)
+
+
+def test_solver_option_validation(small):
+    for bad in [dict(precision=3), dict(starts=0), dict(starts=4), dict(epsilon=0.0), dict(inner=0),
+                dict(threads_per_block=48), dict(resolve_misses=2)]:
+        so = U.solver_options(**bad)
+        with pytest.raises(ValueError):
+            U.unmix_ex(small.image, small.layers, solver=so)
+
+
+def test_too_many_layers_rejected():
+    wl = syn.generate(4, 4, [0] * 9, (2.0, 3.0), seed=1)
+    with pytest.raises(ValueError):
+        U.compute_color_unmixing(wl.image, wl.layers)

@@ -53,7 +53,8 @@ class SolverOptions(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("precision", ctypes.c_int32), ("starts", ctypes.c_int32),
                 ("radius", ctypes.c_int32), ("epsilon", ctypes.c_double), ("resolve_misses", ctypes.c_int32),
                 ("inner", ctypes.c_int32), ("outer", ctypes.c_int32), ("inner_tolerance", ctypes.c_double),
-                ("outer_tolerance", ctypes.c_double), ("threads_per_block", ctypes.c_int32)]
+                ("outer_tolerance", ctypes.c_double), ("threads_per_block", ctypes.c_int32),
+                ("kernel_variant", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -71,9 +72,10 @@ def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> O
 
 
 def solver_options(precision=PRECISION_FP32, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
-                   outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0) -> SolverOptions:
+                   outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0,
+                   kernel_variant=-1) -> SolverOptions:
     return SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
-                         outer, inner_tolerance, outer_tolerance, threads_per_block)
+                         outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant)
 
 
 def _load():

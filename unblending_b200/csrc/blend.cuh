@@ -107,4 +107,57 @@ template <class T> __device__ __forceinline__ void blend_all(int mode, T s, T d,
     }
 }
 
+// Quotient: the FP32 solver uses the fast reciprocal-based division (its
+// results carry FP32 rounding anyway); FP64 keeps IEEE division.
+template <class T> __device__ __forceinline__ T qdiv(T a, T b);
+template <> __device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
+template <> __device__ __forceinline__ double qdiv<double>(double a, double b) { return a / b; }
+
+// Table-driven blend for the FP32 solver: the ten piecewise-bilinear modes
+// without any jump (coefficients selected by a compare), Dodge/Burn/SoftLight
+// behind layer-uniform branches. Same piecewise definitions as blend_all.
+template <class T, class M>
+__device__ __forceinline__ void blend_table(const M& m, int l, T s, T d, T& f, T& fs, T& fd, bool partials) {
+    const int sp = m.special[l];
+    if (sp == 0) {
+        const T t = m.ka[l] * s + m.kb[l] * d + m.kc[l];
+        const bool c = m.strict[l] ? (t < T(0)) : (t <= T(0));
+        const T c0 = c ? m.c0[l][0] : m.c0[l][1];
+        const T cs = c ? m.cs[l][0] : m.cs[l][1];
+        const T cd = c ? m.cd[l][0] : m.cd[l][1];
+        const T csd = c ? m.csd[l][0] : m.csd[l][1];
+        f = c0 + cs * s + cd * d + csd * s * d;
+        if (partials) { fs = cs + csd * d; fd = cd + csd * s; }
+        return;
+    }
+    const T one = T(1), two = T(2), eps = T(1e-5);
+    if (sp == 6) {
+        const T q = one - s;
+        const T v = qdiv(d, q);
+        const bool flat = d < eps || q < eps || one < v;
+        f = d < eps ? T(0) : (q < eps ? one : (v < one ? v : one));
+        if (partials) { fs = flat ? T(0) : qdiv(v, q); fd = flat ? T(0) : qdiv(one, q); }
+    } else if (sp == 7) {
+        const T v = qdiv(one - d, s);
+        const bool flat = one - d < eps || s < eps || one < v;
+        f = one - d < eps ? one : (s < eps ? T(0) : one - (v < one ? v : one));
+        if (partials) { fs = flat ? T(0) : qdiv(v, s); fd = flat ? T(0) : qdiv(one, s); }
+    } else {
+        const bool low = d <= T(0.25);
+        const T r = dsqrt(d);
+        const T g = low ? ((T(16) * d - T(12)) * d + T(4)) * d : r;
+        if (s <= T(0.5)) {
+            f = d - (one - two * s) * d * (one - d);
+            if (partials) { fs = two * d * (one - d); fd = two * s + two * d - T(4) * s * d; }
+        } else {
+            f = d + (two * s - one) * (g - d);
+            if (partials) {
+                const T h = low ? (T(48) * d * d - T(24) * d + T(4)) : qdiv(one, two * r);
+                fs = two * (g - d);
+                fd = one + (two * s - one) * h - (two * s - one);
+            }
+        }
+    }
+}
+
 }  // namespace unb

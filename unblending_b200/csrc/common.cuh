@@ -16,7 +16,42 @@ template <class T> struct Models {
     T prec[kMaxLayers][9];
     int mode[kMaxLayers];
     int X[kMaxLayers], Y[kMaxLayers], Z[kMaxLayers];
+    // Branch-free form of the ten piecewise-bilinear modes:
+    //   B = c0 + cs s + cd d + csd s d, coefficient set [0] where
+    //   t = ka s + kb d + kc satisfies t < 0 (strict) or t <= 0, else set [1];
+    // special = 6, 7, 9 marks Dodge, Burn, SoftLight (evaluated directly).
+    T c0[kMaxLayers][2], cs[kMaxLayers][2], cd[kMaxLayers][2], csd[kMaxLayers][2];
+    T ka[kMaxLayers], kb[kMaxLayers], kc[kMaxLayers];
+    int strict[kMaxLayers], special[kMaxLayers];
 };
+
+// Fills the bilinear table of layer l from its mode (blend_mode.hpp:90-196).
+template <class T> inline void set_blend_table(Models<T>& m, int l, int mode) {
+    auto set = [&](int k, double c0, double cs, double cd, double csd) {
+        m.c0[l][k] = T(c0); m.cs[l][k] = T(cs); m.cd[l][k] = T(cd); m.csd[l][k] = T(csd);
+    };
+    auto both = [&](double c0, double cs, double cd, double csd) { set(0, c0, cs, cd, csd); set(1, c0, cs, cd, csd); };
+    m.ka[l] = T(0); m.kb[l] = T(0); m.kc[l] = T(-1); m.strict[l] = 1; m.special[l] = 0;
+    both(0, 0, 0, 0);
+    switch (mode) {
+    case 0: both(0, 1, 0, 0); break;                                   // normal: s
+    case 1: both(0, 0, 0, 1); break;                                   // multiply: s d
+    case 2: both(0, 1, 1, -1); break;                                  // screen: s + d - s d
+    case 3: m.kb[l] = T(1); m.kc[l] = T(-0.5); m.strict[l] = 0;        // overlay: d <= 1/2
+        set(0, 0, 0, 0, 2); set(1, -1, 2, 2, -2); break;
+    case 4: m.ka[l] = T(1); m.kb[l] = T(-1); m.kc[l] = T(0);           // darken: s < d ? s : d
+        set(0, 0, 1, 0, 0); set(1, 0, 0, 1, 0); break;
+    case 5: m.ka[l] = T(1); m.kb[l] = T(-1); m.kc[l] = T(0);           // lighten: s < d ? d : s
+        set(0, 0, 0, 1, 0); set(1, 0, 1, 0, 0); break;
+    case 8: m.ka[l] = T(1); m.kc[l] = T(-0.5); m.strict[l] = 0;        // hard light: s <= 1/2
+        set(0, 0, 0, 0, 2); set(1, -1, 2, 2, -2); break;
+    case 10: m.ka[l] = T(1); m.kb[l] = T(-1); m.kc[l] = T(0);          // difference: |s - d|
+        set(0, 0, -1, 1, 0); set(1, 0, 1, -1, 0); break;
+    case 11: both(0, 1, 1, -2); break;                                 // exclusion: s + d - 2 s d
+    case 12: both(0, 1, 1, 0); break;                                  // linear dodge: s + d
+    default: m.special[l] = mode; break;                               // 6, 7, 9
+    }
+}
 
 // Solver controls of augmented_lagrangian.cuh:163-167 (history fixed at 6).
 struct SolverControls {

@@ -22,8 +22,21 @@
 // broadcasts; the 3x3 colour prior needs the three deltas of a layer (two
 // shuffles); the adjoint sweep reduces the alpha sensitivities of the three
 // channels once per layer. Every branch is taken on quad-uniform values, so a
-// quad never splits. A persistent grid pulls pixels from an atomic queue,
-// one quad at a time, so slow pixels do not hold up a warp's other quads.
+// quad never splits.
+//
+// Lockstep: the method is run as a state machine in which every step of the
+// warp's loop performs exactly one objective evaluation per quad (the
+// gradient half predicated on the quads that need it), followed by the
+// evaluation-free bookkeeping of that quad's phase (line-search decision,
+// L-BFGS update and two-loop recursion, multiplier update). The eight pixels
+// of a warp therefore share one instruction stream for the expensive part
+// instead of serializing through different phases, and the evaluator has a
+// single call site (one copy in the instruction cache). A quad whose pixel is
+// finished pulls the next pixel from an atomic queue inside the loop; the warp
+// leaves the loop when every quad is idle. The evaluated points and every
+// decision are those of the reference method, step for step; the one
+// evaluation left out is the re-evaluation at the end of an outer step, at a
+// point already evaluated, whose residual the state keeps instead.
 #pragma once
 #include "blend.cuh"
 #include "common.cuh"
@@ -112,86 +125,131 @@ template <class T, int L> struct History<T, L, true> {
     __device__ __forceinline__ void reset() { next = 0; }
 };
 
+enum : int { kIdle = 0, kOuterEval = 1, kTrial = 2, kAcceptGrad = 3 };
+
 template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
+    static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
     const Models<T>& m;
     const SolverControls& ctl;
+    const SolveArgs& a;
     Quad Q;
-    bool opaque, smooth;
-    T tol2;
+    bool colour, opaque, smooth;
+    T tol2, itol;
 
-    // Per-pixel inputs (per lane).
-    T target;            // colour lanes: target channel q
-    T ahat[L];           // lane 3, refinement: filtered alpha targets
-    T lo[L], hi[L];      // variable bounds of this lane's slice
+    // Per-pixel inputs (this lane's slice).
+    size_t pixel;
+    double target64, bg64;
+    T target, bgq;
+    T ahat[R];           // alpha lane, refinement: filtered alpha targets (pinned alphas)
     T init[L];           // start-0 seed before clamping
 
-    // Method state (per lane slice).
+    // Method state (this lane's slice).
     T x[L], g[L], d[L], tr[L], ng[L], ox[L], best[L];
-    T lam[REFINE ? L : 1];   // colour lanes use lam[0]; lane 3 one (unmixing) or L (refinement) rows
-    T res[REFINE ? L : 1];   // residual rows owned by this lane, from the last evaluation
+    T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
     History<T, L, HSMEM> hist;
+
+    // Per-quad scalars (uniform within the quad).
+    int phase, start, outer, it, attempt, bt, valid;
+    T rho, f, oldnorm, step, slope;
     T best_norm, best_energy;
     bool have_best;
     uint32_t n_values, n_gradients, n_iterations, n_backtracks, n_outer;
 
-    __device__ QuadSolver(const Models<T>& models, const SolverControls& c) : m(models), ctl(c) {}
+    __device__ QuadSolver(const Models<T>& models, const SolverControls& c, const SolveArgs& args)
+        : m(models), ctl(c), a(args) {
+        colour = Q.q < 3;
+        opaque = a.opaque != 0;
+        smooth = a.smooth != 0;
+        tol2 = T(ctl.outer_tolerance * ctl.outer_tolerance);
+        itol = T(ctl.inner_tolerance);
+        phase = kIdle;
+    }
+
+    // ------------------------------------------------------------ bounds --
+    __device__ __forceinline__ T lo(int l) const {
+        if (colour) return (REFINE && smooth && l == 0) ? bgq : T(0);
+        if (opaque && l == 0) return T(1);
+        return REFINE ? ahat[REFINE ? l : 0] : T(0);
+    }
+    __device__ __forceinline__ T hi(int l) const {
+        if (colour) return (REFINE && smooth && l == 0) ? bgq : T(1);
+        if (opaque && l == 0) return T(1);
+        return REFINE ? ahat[REFINE ? l : 0] : T(1);
+    }
+    __device__ __forceinline__ T clampb(int l, T v) const {
+        const T lv = lo(l), hv = hi(l);
+        return v < lv ? lv : (v > hv ? hv : v);
+    }
+    __device__ __forceinline__ bool fixed_at(int l, T gl) const {
+        const T lv = lo(l), hv = hi(l);
+        return lv == hv || (x[l] <= lv && gl > T(0)) || (x[l] >= hv && gl < T(0));
+    }
+    __device__ __forceinline__ T mean_of(int l) const {
+        return colour ? sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
+    }
+
+    // FP32: table-driven blend and reciprocal-based division; FP64: the
+    // reference's formulas with IEEE division.
+    static constexpr bool kFast = sizeof(T) == 4;
+    __device__ __forceinline__ T blend(int l, T s, T d) const {
+        if constexpr (kFast) { T f, fs, fd; blend_table<T>(m, l, s, d, f, fs, fd, false); return f; }
+        else return blend_value<T>(m.mode[l], s, d);
+    }
+    __device__ __forceinline__ void blend3(int l, T s, T d, T& f, T& fs, T& fd) const {
+        if constexpr (kFast) blend_table<T>(m, l, s, d, f, fs, fd, true);
+        else blend_all<T>(m.mode[l], s, d, f, fs, fd);
+    }
+
+    // sy > 1e-9 sqrt(ss yy) and sy > 0 (augmented_lagrangian.cuh:193,290); the
+    // FP32 solver compares squares instead of taking the root.
+    __device__ __forceinline__ static bool curvature_ok(T sy, T ss, T yy) {
+        if constexpr (kFast) return sy > T(0) && sy * sy > T(1e-18) * (ss * yy);
+        else return sy > T(1e-9) * dsqrt(ss * yy) && sy > T(0);
+    }
 
     // ---------------------------------------------------------- evaluate --
-    // AL value E + sum(rho/2 C^2 - lambda C), uniform across the quad. Sets
-    // res[], returns energy E and |C|^2 (uniform) and, if DERIV, the gradient
-    // slice `gr`. Tracks the best feasible point.
-    template <bool DERIV> __device__ __forceinline__ T evaluate(const T* pt, T rho, T* gr) {
-        ++n_values;
-        if (DERIV) ++n_gradients;
-        const bool colour = Q.q < 3;
-        T a[L], A[L], pc[L];
+    // Evaluates the AL value at tr (uniform across the quad), sets res[] and,
+    // when need_grad, the gradient slice ng[]. Tracks the best feasible point.
+    __device__ __forceinline__ T evaluate(bool need_grad, bool active) {
+        T al[L], A[L], pc[L];
 #pragma unroll
-        for (int l = 0; l < L; ++l) a[l] = Q.from(pt[l], 3);
-        // Forward composite, bottom to top. pc[l] = this channel after layer l.
-        A[0] = a[0];
-        pc[0] = pt[0];
+        for (int l = 0; l < L; ++l) al[l] = Q.from(tr[l], 3);
+        A[0] = al[0];
+        pc[0] = tr[0];
 #pragma unroll
         for (int l = 1; l < L; ++l) {
-            const T al = a[l], dd = A[l - 1];
-            const T Al = T(m.X[l]) * al * dd + T(m.Y[l]) * al * (T(1) - dd) + T(m.Z[l]) * dd * (T(1) - al);
+            const T av = al[l], dd = A[l - 1];
+            const T Al = T(m.X[l]) * av * dd + T(m.Y[l]) * av * (T(1) - dd) + T(m.Z[l]) * dd * (T(1) - av);
             A[l] = Al;
-            const T s = pt[l], c = pc[l - 1];
-            const T pre = blend_value<T>(m.mode[l], s, c) * al * dd + T(m.Y[l]) * al * (T(1) - dd) * s +
-                          T(m.Z[l]) * dd * (T(1) - al) * c;
-            pc[l] = Al > T(1e-12) ? pre / Al : pre;
+            const T s = tr[l], c = pc[l - 1];
+            const T pre = blend(l, s, c) * av * dd + T(m.Y[l]) * av * (T(1) - dd) * s +
+                          T(m.Z[l]) * dd * (T(1) - av) * c;
+            pc[l] = Al > T(1e-12) ? qdiv(pre, Al) : pre;
         }
-        // Colour prior: every lane gathers the three deltas of each layer.
-        T energy = T(0), asum = T(0), D[L];
+        T energy = T(0), asum = T(0);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const T mine = colour ? pt[l] - sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
+            const T mine = colour ? tr[l] - mean_of(l) : T(0);
             const T d0 = Q.from(mine, 0), d1 = Q.from(mine, 1), d2 = Q.from(mine, 2);
             const T* P = m.prec[l];
             const T v0 = P[0] * d0 + P[1] * d1 + P[2] * d2;
             const T v1 = P[3] * d0 + P[4] * d1 + P[5] * d2;
             const T v2 = P[6] * d0 + P[7] * d1 + P[8] * d2;
-            D[l] = d0 * v0 + d1 * v1 + d2 * v2;
-            energy += a[l] * D[l];
-            asum += a[l];
-            if (DERIV) {
+            const T D = d0 * v0 + d1 * v1 + d2 * v2;
+            energy += al[l] * D;
+            asum += al[l];
+            if (need_grad) {
                 if (colour) {
-                    // (P + P^T) delta, row q.
-                    const T vq = Q.q == 0 ? v0 : (Q.q == 1 ? v1 : v2);
+                    const T vq = sel3(Q.q, v0, v1, v2);
                     const T tq = sel3(Q.q, P[0], P[1], P[2]) * d0 + sel3(Q.q, P[3], P[4], P[5]) * d1 +
                                  sel3(Q.q, P[6], P[7], P[8]) * d2;
-                    gr[l] = a[l] * (vq + tq);
+                    ng[l] = al[l] * (vq + tq);
                 } else {
-                    gr[l] = D[l];
+                    ng[l] = D + (REFINE ? T(0) : T(0.01));
                 }
             }
         }
-        if (!REFINE) {
-            energy += T(0.01) * asum;
-            if (DERIV && !colour)
-#pragma unroll
-                for (int l = 0; l < L; ++l) gr[l] += T(0.01);
-        }
-        // Residual rows and AL terms owned by this lane.
+        if (!REFINE) energy += T(0.01) * asum;
         T terms = T(0), norm = T(0);
         if (colour) {
             res[0] = pc[L - 1] - target;
@@ -199,8 +257,8 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
             norm = res[0] * res[0];
         } else if (REFINE) {
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-                res[l] = pt[l] - ahat[l];
+            for (int l = 0; l < R; ++l) {
+                res[l] = tr[l] - ahat[l];
                 terms += T(0.5) * rho * res[l] * res[l] - lam[l] * res[l];
                 norm += res[l] * res[l];
             }
@@ -211,72 +269,78 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
         }
         Q.sum2(terms, norm);
         const T value = energy + terms;
-        // Best-feasible tracking (augmented_lagrangian.cuh:237-240).
-        const bool feasible = norm < tol2;
-        if (finite_(energy) && finite_(norm) &&
-            (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
-             (!feasible && best_norm >= tol2 && norm < best_norm))) {
-            have_best = true; best_norm = norm; best_energy = energy;
+        if (active) {
+            ++n_values;
+            if (need_grad) ++n_gradients;
+            const bool feasible = norm < tol2;
+            if (finite_(energy) && finite_(norm) &&
+                (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
+                 (!feasible && best_norm >= tol2 && norm < best_norm))) {
+                have_best = true; best_norm = norm; best_energy = energy;
 #pragma unroll
-            for (int l = 0; l < L; ++l) best[l] = pt[l];
-        }
-        if (!DERIV) return value;
-
-        // Reverse sweep. adj: this channel's cotangent; adj3: the alpha chain's.
-        T adj = colour ? rho * res[0] - lam[0] : T(0);
-        T adj3 = (!colour && !REFINE) ? rho * res[0] - lam[0] : T(0);
-        if (REFINE && !colour)
-#pragma unroll
-            for (int l = 0; l < L; ++l) gr[l] += rho * res[l] - lam[l];
-#pragma unroll
-        for (int l = L - 1; l > 0; --l) {
-            const T al = a[l], dd = A[l - 1], Al = A[l];
-            const T X = T(m.X[l]), Y = T(m.Y[l]), Z = T(m.Z[l]);
-            const T da = X * dd + Y * (T(1) - dd) - Z * dd;
-            const T db = X * al - Y * al + Z * (T(1) - al);
-            const bool big = Al > T(1e-12);
-            T ga, gp;
-            if (colour) {
-                const T s = pt[l], c = pc[l - 1], out = pc[l], v = adj;
-                T f, fs, fd;
-                blend_all<T>(m.mode[l], s, c, f, fs, fd);
-                const T ds = al * dd * fs + Y * al * (T(1) - dd);
-                const T dc = al * dd * fd + Z * dd * (T(1) - al);
-                const T pa = f * dd + Y * (T(1) - dd) * s - Z * dd * c;
-                const T pd = f * al - Y * al * s + Z * (T(1) - al) * c;
-                if (big) {
-                    const T inv = T(1) / Al;
-                    ga = v * ((pa - out * da) * inv);
-                    gp = v * ((pd - out * db) * inv);
-                    if (DERIV) gr[l] += v * (ds * inv);
-                    adj = v * (dc * inv);
-                } else {
-                    ga = v * pa; gp = v * pd;
-                    gr[l] += v * ds;
-                    adj = v * dc;
-                }
-            } else {
-                ga = adj3 * da;
-                gp = adj3 * db;
+                for (int l = 0; l < L; ++l) best[l] = tr[l];
             }
-            Q.sum2(ga, gp);
-            if (!colour) { gr[l] += ga; adj3 = gp; }
         }
-        gr[0] += colour ? adj : adj3;
+        if (need_grad) {
+            T adj = colour ? rho * res[0] - lam[0] : T(0);
+            T adj3 = (!colour && !REFINE) ? rho * res[0] - lam[0] : T(0);
+            if (REFINE && !colour)
+#pragma unroll
+                for (int l = 0; l < R; ++l) ng[l] += rho * res[l] - lam[l];
+#pragma unroll
+            for (int l = L - 1; l > 0; --l) {
+                const T av = al[l], dd = A[l - 1], Al = A[l];
+                const T X = T(m.X[l]), Y = T(m.Y[l]), Z = T(m.Z[l]);
+                const T da = X * dd + Y * (T(1) - dd) - Z * dd;
+                const T db = X * av - Y * av + Z * (T(1) - av);
+                const bool big = Al > T(1e-12);
+                T ga, gp;
+                if (colour) {
+                    const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
+                    T fv, fs, fd;
+                    blend3(l, s, c, fv, fs, fd);
+                    const T ds = av * dd * fs + Y * av * (T(1) - dd);
+                    const T dc = av * dd * fd + Z * dd * (T(1) - av);
+                    const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
+                    const T pd = fv * av - Y * av * s + Z * (T(1) - av) * c;
+                    if (big) {
+                        if constexpr (kFast) {
+                            const T r = qdiv(T(1), Al);
+                            ga = v * ((pa - out * da) * r);
+                            gp = v * ((pd - out * db) * r);
+                            ng[l] += v * (ds * r);
+                            adj = v * (dc * r);
+                        } else {
+                            ga = v * ((pa - out * da) / Al);
+                            gp = v * ((pd - out * db) / Al);
+                            ng[l] += v * (ds / Al);
+                            adj = v * (dc / Al);
+                        }
+                    } else {
+                        ga = v * pa; gp = v * pd;
+                        ng[l] += v * ds;
+                        adj = v * dc;
+                    }
+                } else {
+                    ga = adj3 * da;
+                    gp = adj3 * db;
+                }
+                Q.sum2(ga, gp);
+                if (!colour) { ng[l] += ga; adj3 = gp; }
+            }
+            ng[0] += colour ? adj : adj3;
+        }
         return value;
     }
 
-    // ------------------------------------------------------------ helpers --
-    __device__ __forceinline__ bool fixed_at(int l, T gl) const {
-        return lo[l] == hi[l] || (x[l] <= lo[l] && gl > T(0)) || (x[l] >= hi[l] && gl < T(0));
-    }
+    // ------------------------------------------------------ bookkeeping --
     __device__ __forceinline__ void steepest() {
 #pragma unroll
         for (int l = 0; l < L; ++l) d[l] = fixed_at(l, g[l]) ? T(0) : -g[l];
     }
 
     // Two-loop recursion on the current free set; d holds q on entry/exit.
-    __device__ __forceinline__ void two_loop(int valid, const bool* freev) {
+    __device__ __forceinline__ void two_loop(const bool* freev) {
         T coeff[kHistory], inv[kHistory];
         T scaling = T(1);
         bool have_scaling = false;
@@ -287,17 +351,17 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
 #pragma unroll
                 for (int l = 0; l < L; ++l)
                     if (freev[l]) {
-                        const T a = hist.s(j, l), b = hist.y(j, l);
-                        dot += a * d[l]; sy += a * b; ss += a * a; yy += b * b;
+                        const T sa = hist.s(j, l), yb = hist.y(j, l);
+                        dot += sa * d[l]; sy += sa * yb; ss += sa * sa; yy += yb * yb;
                     }
                 Q.sum4(dot, sy, ss, yy);
-                const T r = T(1) / sy;
-                inv[j] = (sy > T(1e-9) * dsqrt(ss * yy) && sy > T(0) && finite_(r)) ? r : T(0);
+                const T r = qdiv(T(1), sy);
+                inv[j] = (curvature_ok(sy, ss, yy) && finite_(r)) ? r : T(0);
                 coeff[j] = dot * inv[j];
 #pragma unroll
                 for (int l = 0; l < L; ++l)
                     if (freev[l]) d[l] -= coeff[j] * hist.y(j, l);
-                if (!have_scaling && inv[j] > T(0) && yy > T(0)) { scaling = sy / yy; have_scaling = true; }
+                if (!have_scaling && inv[j] > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             }
         }
         scaling = fmax(T(1e-12), fmin(T(1e3), scaling));
@@ -311,173 +375,330 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
                 for (int l = 0; l < L; ++l)
                     if (freev[l]) dot += hist.y(j, l) * d[l];
                 dot = Q.sum(dot);
-                const T a = coeff[j] - dot * inv[j];
+                const T c = coeff[j] - dot * inv[j];
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) d[l] += a * hist.s(j, l);
+                    if (freev[l]) d[l] += c * hist.s(j, l);
             }
         }
     }
 
-    __device__ __forceinline__ T mean_of(int l) const {
-        return Q.q < 3 ? sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
-    }
-    __device__ __forceinline__ T clampb(int l, T v) const { return v < lo[l] ? lo[l] : (v > hi[l] ? hi[l] : v); }
-
-    // Starting point `start` (augmented_lagrangian.cuh:243-263).
-    __device__ __forceinline__ void seed(int start) {
-        const bool colour = Q.q < 3;
+    // Starting point `s` (augmented_lagrangian.cuh:243-263); ends ready to
+    // evaluate the first outer step.
+    __device__ __forceinline__ void begin_start(int s) {
+        start = s;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
             T v = init[l];
-            if (!REFINE && start == 1) {
+            if (!REFINE && s == 1) {
                 if (!colour) v = l == 0 ? T(1) : T(0);
                 else v = l == 0 ? fmin(T(1), fmax(T(0), target)) : mean_of(l);
             }
-            if (REFINE && start && colour) v = mean_of(l);
-            if (start == 2) {
+            if (REFINE && s && colour) v = mean_of(l);
+            if (s == 2) {
                 if (!colour) v = REFINE ? init[l] : T(0.5);
                 else v = fmax(T(0.05), fmin(T(0.95), mean_of(l)));
             }
-            x[l] = v < lo[l] ? lo[l] : (v > hi[l] ? hi[l] : v);
+            x[l] = clampb(l, v);
         }
-        if (start == 2) {
+        if (s == 2) {
             // Move Dodge/Burn sources into the unsaturated branch.
-            T a[L];
+            T av[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) a[l] = Q.from(x[l], 3);
-            T dest = x[0], da = a[0];
+            for (int l = 0; l < L; ++l) av[l] = Q.from(x[l], 3);
+            T dest = x[0], da = av[0];
 #pragma unroll
             for (int l = 1; l < L; ++l) {
-                const T al = a[l];
+                const T al = av[l];
                 const T Al = T(m.X[l]) * al * da + T(m.Y[l]) * al * (T(1) - da) + T(m.Z[l]) * da * (T(1) - al);
                 if (colour) {
-                    T s = x[l];
-                    if (dest >= T(0) && dest <= T(1) && m.mode[l] == 6) s = fmin(s, fmax(T(0), T(1) - dest - T(0.05)));
-                    if (dest >= T(0) && dest <= T(1) && m.mode[l] == 7) s = fmax(s, fmin(T(1), T(1) - dest + T(0.05)));
-                    s = clampb(l, s);
-                    x[l] = s;
-                    const T pre = blend_value<T>(m.mode[l], s, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * s +
+                    T sv = x[l];
+                    if (dest >= T(0) && dest <= T(1) && m.mode[l] == 6) sv = fmin(sv, fmax(T(0), T(1) - dest - T(0.05)));
+                    if (dest >= T(0) && dest <= T(1) && m.mode[l] == 7) sv = fmax(sv, fmin(T(1), T(1) - dest + T(0.05)));
+                    sv = clampb(l, sv);
+                    x[l] = sv;
+                    const T pre = blend_value<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
                                   T(m.Z[l]) * da * (T(1) - al) * dest;
                     dest = Al > T(1e-12) ? pre / Al : pre;
                 }
                 da = Al;
             }
         }
+#pragma unroll
+        for (int r = 0; r < R; ++r) lam[r] = T(0);
+        rho = T(100);
+        outer = 0;
+        begin_outer();
     }
 
-    // --------------------------------------------------------------- solve --
-    __device__ void run() {
+    __device__ __forceinline__ void begin_outer() {
+        ++n_outer;
+#pragma unroll
+        for (int l = 0; l < L; ++l) { ox[l] = x[l]; tr[l] = x[l]; }
+        phase = kOuterEval;
+    }
+
+    __device__ __forceinline__ T own_norm(const T* r) const {
+        if (colour || !REFINE) return r[0] * r[0];
+        T s = T(0);
+#pragma unroll
+        for (int l = 0; l < R; ++l) s += r[l] * r[l];
+        return s;
+    }
+
+    // End of an outer step: multiplier and penalty update from the residual
+    // at x, then the next outer step, the next start, or done (phase kIdle
+    // with have_best set: the caller writes the pixel).
+    __device__ __forceinline__ void end_outer() {
+        const T norm = Q.sum(own_norm(resx));
+        const bool feasible = norm < tol2;
+#pragma unroll
+        for (int r = 0; r < R; ++r) lam[r] -= rho * resx[r];
+        if (norm > T(0.0625) * oldnorm) rho *= T(10);
+        T motion = T(0);
+#pragma unroll
+        for (int l = 0; l < L; ++l) { const T dl = x[l] - ox[l]; motion += dl * dl; }
+        motion = Q.sum(motion);
+        if (!(motion < tol2 && feasible) && outer + 1 < ctl.outer) {
+            ++outer;
+            begin_outer();
+        } else if (start + 1 < ctl.starts) {
+            begin_start(start + 1);
+        } else {
+            phase = kIdle;
+        }
+    }
+
+    // Finds the next line-search trial point with non-zero motion (phase
+    // kTrial), or ends the inner solve when both attempts are exhausted.
+    __device__ __forceinline__ void next_trial() {
+        for (;;) {
+            if (bt < 32) {
+                T sl = T(0), mo = T(0);
+#pragma unroll
+                for (int l = 0; l < L; ++l) {
+                    tr[l] = clampb(l, x[l] + step * d[l]);
+                    const T delta = tr[l] - x[l];
+                    sl += g[l] * delta;
+                    mo += delta * delta;
+                }
+                Q.sum2(sl, mo);
+                if (mo != T(0)) { slope = sl; phase = kTrial; return; }
+            }
+            // This attempt failed: restart from steepest descent once.
+            valid = 0; hist.reset(); steepest();
+            if (attempt == 0) { attempt = 1; bt = 0; step = T(1); continue; }
+            end_outer();
+            return;
+        }
+    }
+
+    // Top of an inner iteration: projected gradient test, two-loop
+    // direction, first trial.
+    __device__ __forceinline__ void begin_iteration() {
+        ++n_iterations;
+        bool freev[L];
+        T pg2 = T(0);
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            freev[l] = !fixed_at(l, g[l]);
+            d[l] = freev[l] ? g[l] : T(0);
+            pg2 += d[l] * d[l];
+        }
+        pg2 = Q.sum(pg2);
+        if (pg2 < T(1e-16) || !finite_(f)) { end_outer(); return; }
+        two_loop(freev);
+        T descent = T(0);
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            T v = -d[l];
+            const T lv = lo(l), hv = hi(l);
+            if (lv == hv || (x[l] <= lv && v < T(0)) || (x[l] >= hv && v > T(0))) v = T(0);
+            d[l] = v;
+            descent += v * g[l];
+        }
+        descent = Q.sum(descent);
+        if (!(descent < T(0))) { valid = 0; hist.reset(); steepest(); }
+        attempt = 0; bt = 0; step = T(1);
+        next_trial();
+    }
+
+    // Accepted step: curvature pair, move, inner termination test.
+    __device__ __forceinline__ void accept(T cand) {
+        T sy = T(0), ss = T(0), yy = T(0), mm = T(0);
+        T sv[L], yv[L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            sv[l] = tr[l] - x[l];
+            yv[l] = ng[l] - g[l];
+            sy += sv[l] * yv[l]; ss += sv[l] * sv[l]; yy += yv[l] * yv[l];
+            mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(x[l])));
+        }
+        Q.sum3(sy, ss, yy);
+        mm = Q.max(mm);
+        const T r = qdiv(T(1), sy);
+        if (curvature_ok(sy, ss, yy) && finite_(r)) {
+            hist.push(sv, yv);
+            valid = valid + 1 < kHistory ? valid + 1 : kHistory;
+        }
+        const T delta = fabs(f - cand), size = T(0.5) * (fabs(f) + fabs(cand));
+#pragma unroll
+        for (int l = 0; l < L; ++l) { x[l] = tr[l]; g[l] = ng[l]; }
+#pragma unroll
+        for (int q = 0; q < R; ++q) resx[q] = res[q];
+        f = cand;
+        if (delta < itol * size || mm < itol) { end_outer(); return; }
+        if (++it >= ctl.inner) { end_outer(); return; }
+        begin_iteration();
+    }
+
+    // ------------------------------------------------------------ pixels --
+    // Loads pixel `i` and prepares start 0.
+    __device__ __forceinline__ void load(size_t i) {
+        const size_t n = size_t(a.n);
+        pixel = i;
+        target64 = colour ? a.image[3 * i + Q.q] : 0.0;
+        target = T(target64);
+        bg64 = (REFINE && smooth && colour) ? a.targets[(size_t(L) + Q.q) * n + i] : 0.0;
+        bgq = T(bg64);
+#pragma unroll
+        for (int l = 0; l < R; ++l) {
+            double t = REFINE ? a.targets[size_t(l) * n + i] : 0.0;
+            if (REFINE && opaque && l == 0) t = 1.0;
+            ahat[l] = T(t);
+        }
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            if (colour) {
+                if (REFINE) init[l] = (smooth && l == 0) ? bgq : T(a.first[(size_t(l) * n + i) * 4 + Q.q]);
+                else init[l] = fmin(T(1), fmax(T(0), mean_of(l)));
+            } else {
+                init[l] = (opaque && l == 0) ? T(1) : (REFINE ? ahat[REFINE ? l : 0] : T(0.5));
+            }
+        }
         have_best = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);
         n_values = n_gradients = n_iterations = n_backtracks = n_outer = 0;
-        const T itol = T(ctl.inner_tolerance);
-        for (int start = 0; start < ctl.starts; ++start) {
-            seed(start);
+        begin_start(0);
+    }
+
+    // Writes the finished pixel: output (pinned values exactly), FP64
+    // feasibility check, status, miss list, counters.
+    __device__ __forceinline__ void store(bool skipped) {
+        const size_t n = size_t(a.n), i = pixel;
+        double v[L], ah[R];
 #pragma unroll
-            for (int r = 0; r < (REFINE ? L : 1); ++r) lam[r] = T(0);
-            T rho = T(100);
-            for (int outer = 0; outer < ctl.outer; ++outer) {
-                ++n_outer;
+        for (int l = 0; l < R; ++l) {
+            double t = REFINE ? a.targets[size_t(l) * n + i] : 0.0;
+            if (REFINE && opaque && l == 0) t = 1.0;
+            ah[l] = t;
+        }
 #pragma unroll
-                for (int l = 0; l < L; ++l) ox[l] = x[l];
-                T f = evaluate<true>(x, rho, g);
-                T oldnorm = Q.sum(own_norm());
-                int valid = 0;
-                hist.reset();
-                for (int it = 0; it < ctl.inner; ++it) {
-                    ++n_iterations;
-                    bool freev[L];
-                    T pg2 = T(0);
+        for (int l = 0; l < L; ++l) {
+            v[l] = double(have_best ? best[l] : init[l]);
+            if (REFINE && !colour) v[l] = ah[REFINE ? l : 0];
+            if (REFINE && smooth && colour && l == 0) v[l] = bg64;
+            if (!REFINE && opaque && !colour && l == 0) v[l] = 1.0;
+            a.out[(size_t(l) * n + i) * 4 + Q.q] = v[l];
+        }
+        // FP64 constraint check of the written point (solver_workspace.cuh:18-38).
+        double av[L];
 #pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        freev[l] = !fixed_at(l, g[l]);
-                        d[l] = freev[l] ? g[l] : T(0);
-                        pg2 += d[l] * d[l];
-                    }
-                    pg2 = Q.sum(pg2);
-                    if (pg2 < T(1e-16) || !finite_(f)) break;
-                    two_loop(valid, freev);
-                    T descent = T(0);
+        for (int l = 0; l < L; ++l) av[l] = Q.from(v[l], 3);
+        double A = av[0], c = v[0];
 #pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        T v = -d[l];
-                        if (lo[l] == hi[l] || (x[l] <= lo[l] && v < T(0)) || (x[l] >= hi[l] && v > T(0))) v = T(0);
-                        d[l] = v;
-                        descent += v * g[l];
-                    }
-                    descent = Q.sum(descent);
-                    if (!(descent < T(0))) { valid = 0; hist.reset(); steepest(); }
-                    bool accepted = false, have_grad = false;
-                    T cand = f;
-                    for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
-                        T step = T(1);
-                        for (int bt = 0; bt < 32; ++bt) {
-                            T slope = T(0), motion = T(0);
+        for (int l = 1; l < L; ++l) {
+            const double al = av[l], dd = A;
+            const double Al = double(m.X[l]) * al * dd + double(m.Y[l]) * al * (1.0 - dd) +
+                              double(m.Z[l]) * dd * (1.0 - al);
+            const double s = v[l];
+            const double pre = blend_value<double>(m.mode[l], s, c) * al * dd + double(m.Y[l]) * al * (1.0 - dd) * s +
+                               double(m.Z[l]) * dd * (1.0 - al) * c;
+            c = Al > 1e-12 ? pre / Al : pre;
+            A = Al;
+        }
+        double norm = 0.0;
+        if (colour) { const double r = c - target64; norm = r * r; }
+        else if (REFINE) {
 #pragma unroll
-                            for (int l = 0; l < L; ++l) {
-                                tr[l] = clampb(l, x[l] + step * d[l]);
-                                const T delta = tr[l] - x[l];
-                                slope += g[l] * delta;
-                                motion += delta * delta;
-                            }
-                            Q.sum2(slope, motion);
-                            if (motion == T(0)) break;
-                            ++n_backtracks;
-                            if (bt == 0 && ctl.gradient_on_first_trial) { cand = evaluate<true>(tr, rho, ng); have_grad = true; }
-                            else { cand = evaluate<false>(tr, rho, ng); have_grad = false; }
-                            if (slope < T(0) && finite_(cand) && cand <= f + T(1e-4) * slope) { accepted = true; break; }
-                            step *= T(0.5);
-                        }
-                        if (!accepted) { valid = 0; hist.reset(); steepest(); }
-                    }
-                    if (!accepted) break;
-                    if (!have_grad) cand = evaluate<true>(tr, rho, ng);
-                    T sy = T(0), ss = T(0), yy = T(0), mm = T(0);
-                    T sv[L], yv[L];
-#pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        sv[l] = tr[l] - x[l];
-                        yv[l] = ng[l] - g[l];
-                        sy += sv[l] * yv[l]; ss += sv[l] * sv[l]; yy += yv[l] * yv[l];
-                        mm = fmax(mm, fabs(sv[l]) / (T(1) + fabs(x[l])));
-                    }
-                    Q.sum3(sy, ss, yy);
-                    mm = Q.max(mm);
-                    const T r = T(1) / sy;
-                    if (sy > T(1e-9) * dsqrt(ss * yy) && sy > T(0) && finite_(r)) {
-                        hist.push(sv, yv);
-                        valid = valid + 1 < kHistory ? valid + 1 : kHistory;
-                    }
-                    const T delta = fabs(f - cand), size = T(0.5) * (fabs(f) + fabs(cand));
-#pragma unroll
-                    for (int l = 0; l < L; ++l) { x[l] = tr[l]; g[l] = ng[l]; }
-                    f = cand;
-                    if (delta < itol * size || mm < itol) break;
-                }
-                f = evaluate<true>(x, rho, g);
-                const T norm = Q.sum(own_norm());
-                const bool feasible = norm < tol2;
-#pragma unroll
-                for (int r = 0; r < (REFINE ? L : 1); ++r) lam[r] -= rho * res[r];
-                if (norm > T(0.0625) * oldnorm) rho *= T(10);
-                T motion = T(0);
-#pragma unroll
-                for (int l = 0; l < L; ++l) { const T dl = x[l] - ox[l]; motion += dl * dl; }
-                motion = Q.sum(motion);
-                if (motion < tol2 && feasible) break;
+            for (int l = 0; l < R; ++l) { const double r = v[l] - ah[l]; norm += r * r; }
+        } else { const double r = A - 1.0; norm = r * r; }
+        norm = Q.sum(norm);
+        const bool miss = !(norm < ctl.outer_tolerance * ctl.outer_tolerance);
+        if (Q.q == 0) {
+            if (skipped) {
+                if (a.status) a.status[i] = 8;
+                if (a.input_failed) atomicAdd(a.input_failed, 1);
+            } else {
+                if (a.status) a.status[i] = miss ? 3 : 0;
+                if (miss && a.miss_list) a.miss_list[atomicAdd(a.miss_count, 1)] = int32_t(i);
+            }
+            if (a.counters) {
+                uint32_t* cnt = a.counters + 5 * i;
+                cnt[0] = n_values; cnt[1] = n_gradients; cnt[2] = n_iterations; cnt[3] = n_backtracks; cnt[4] = n_outer;
             }
         }
     }
 
-    // |C|^2 contribution of the residual rows owned by this lane (res[] of
-    // the last evaluation).
-    __device__ __forceinline__ T own_norm() const {
-        if (Q.q < 3 || !REFINE) return res[0] * res[0];
-        T s = T(0);
+    // Pulls pixels until one needs solving (phase != kIdle) or the queue is
+    // empty (phase kIdle, returns false).
+    __device__ __forceinline__ bool fetch(int total) {
+        for (;;) {
+            int job = 0;
+            if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
+            job = Q.from(job, 0);
+            if (job >= total) { phase = kIdle; return false; }
+            const size_t i = size_t(a.list ? a.list[job] : job);
+            load(i);
+            if (REFINE && a.input_status && a.input_status[i] != 0) {
+                // Targets that cannot be normalized: keep the initial layers
+                // and report status 8 (solver_workspace.cuh:144).
+                have_best = false;
+                n_values = n_gradients = n_iterations = n_backtracks = n_outer = 0;
+                store(true);
+                continue;
+            }
+            return true;
+        }
+    }
+
+    // ------------------------------------------------------------- loop --
+    __device__ void run() {
+        const int total = a.list ? *a.list_count : a.n;
+        bool live = fetch(total);
+        for (;;) {
+            if (__all_sync(0xffffffffu, !live)) break;
+            const bool need_grad = phase == kOuterEval || phase == kAcceptGrad ||
+                                   (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial);
+            const T value = evaluate(need_grad && live, live);
+            if (!live) continue;
+            if (phase == kOuterEval) {
+                f = value;
 #pragma unroll
-        for (int l = 0; l < L; ++l) s += res[l] * res[l];
-        return s;
+                for (int l = 0; l < L; ++l) g[l] = ng[l];
+#pragma unroll
+                for (int q = 0; q < R; ++q) resx[q] = res[q];
+                oldnorm = Q.sum(own_norm(res));
+                valid = 0; hist.reset(); it = 0;
+                begin_iteration();
+            } else if (phase == kTrial) {
+                ++n_backtracks;
+                if (slope < T(0) && finite_(value) && value <= f + T(1e-4) * slope) {
+                    if (need_grad) accept(value);
+                    else phase = kAcceptGrad;
+                } else {
+                    step *= T(0.5);
+                    ++bt;
+                    next_trial();
+                }
+            } else {   // kAcceptGrad
+                accept(value);
+            }
+            if (phase == kIdle) {
+                store(false);
+                live = fetch(total);
+            }
+        }
     }
 };
 

@@ -6,8 +6,9 @@ namespace unb {
 
 // Persistent solve over SolveArgs::n pixels (or SolveArgs::list); the grid
 // is `threads`-wide blocks times the occupancy limit times `sms`.
-cudaError_t launch_solve_fp32(int L, bool refine, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
-                              int threads, int sms, cudaStream_t s);
+// variant 0: L-BFGS history in registers; 1: in shared memory.
+cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<float>& m, const SolverControls& c,
+                              const SolveArgs& a, int threads, int sms, cudaStream_t s);
 cudaError_t launch_solve_fp64(int L, bool refine, const Models<double>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
 

@@ -1,38 +1,42 @@
-// FP32 instantiations of the per-pixel solve (history in registers).
+// FP32 instantiations of the per-pixel solve. Variant 0 keeps the L-BFGS
+// history in registers (fewer, fatter warps); variant 1 keeps it in shared
+// memory and caps registers for four 128-thread blocks per SM.
 #include "solver_dispatch.hpp"
 #include "solver_kernels.cuh"
 
 namespace unb {
 
 namespace {
-template <int L, bool R> cudaError_t go(const Models<float>& m, const SolverControls& c, const SolveArgs& a,
-                                         int threads, int sms, cudaStream_t s) {
-    using Launch = SolveLauncher<float, L, R, false>;
+template <int L, bool R, bool H> cudaError_t go(const Models<float>& m, const SolverControls& c, const SolveArgs& a,
+                                                int threads, int sms, cudaStream_t s) {
+    using Launch = SolveLauncher<float, L, R, H>;
     int per_sm = 0;
     cudaError_t e = Launch::occupancy(threads, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     return Launch::launch(m, c, a, per_sm * sms, threads, s);
 }
-template <bool R> cudaError_t pick(int L, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
-                                   int threads, int sms, cudaStream_t s) {
+template <bool R, bool H> cudaError_t pick(int L, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
+                                           int threads, int sms, cudaStream_t s) {
     switch (L) {
-    case 1: return go<1, R>(m, c, a, threads, sms, s);
-    case 2: return go<2, R>(m, c, a, threads, sms, s);
-    case 3: return go<3, R>(m, c, a, threads, sms, s);
-    case 4: return go<4, R>(m, c, a, threads, sms, s);
-    case 5: return go<5, R>(m, c, a, threads, sms, s);
-    case 6: return go<6, R>(m, c, a, threads, sms, s);
-    case 7: return go<7, R>(m, c, a, threads, sms, s);
-    case 8: return go<8, R>(m, c, a, threads, sms, s);
+    case 1: return go<1, R, H>(m, c, a, threads, sms, s);
+    case 2: return go<2, R, H>(m, c, a, threads, sms, s);
+    case 3: return go<3, R, H>(m, c, a, threads, sms, s);
+    case 4: return go<4, R, H>(m, c, a, threads, sms, s);
+    case 5: return go<5, R, H>(m, c, a, threads, sms, s);
+    case 6: return go<6, R, H>(m, c, a, threads, sms, s);
+    case 7: return go<7, R, H>(m, c, a, threads, sms, s);
+    case 8: return go<8, R, H>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
 }  // namespace
 
-cudaError_t launch_solve_fp32(int L, bool refine, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
-                              int threads, int sms, cudaStream_t s) {
-    return refine ? pick<true>(L, m, c, a, threads, sms, s) : pick<false>(L, m, c, a, threads, sms, s);
+cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<float>& m, const SolverControls& c,
+                              const SolveArgs& a, int threads, int sms, cudaStream_t s) {
+    if (variant == 1)
+        return refine ? pick<true, true>(L, m, c, a, threads, sms, s) : pick<false, true>(L, m, c, a, threads, sms, s);
+    return refine ? pick<true, false>(L, m, c, a, threads, sms, s) : pick<false, false>(L, m, c, a, threads, sms, s);
 }
 
 }  // namespace unb
