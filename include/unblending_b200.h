@@ -87,6 +87,29 @@ UNBLENDING_API int32_t unblending_refine_device(
     const double* first_pass, const unblending_options* options, const unblending_solver_options* solver,
     double* output, int32_t* status, uint32_t* counters, void* stream, unblending_stats* stats);
 
+/* First pass that allocates nothing. No counterpart in the reference: it
+ * exists for callers that must not allocate device memory inside their
+ * processing call, such as a host application that owns all device memory
+ * through its own allocator, or a per-frame effect whose time budget cannot
+ * absorb cudaMalloc/cudaFree (both can synchronize the device).
+ *
+ * Same arguments and results as unblending_unmix_device without counters and
+ * stats; the caller still passes the input image, output and optional status
+ * buffers (device memory). The solve's scratch (queue heads, miss counters,
+ * miss lists) lives in a fixed 32 MiB + 256 B device array that every GPU
+ * loading the library holds until the process exits; images larger than
+ * 2048 * 2048 = 4,194,304 pixels return UNBLENDING_INVALID_ARGUMENT. The call
+ * uses no cudaMalloc, cudaFree, library stream or event; work is enqueued on
+ * `stream` (NULL: the legacy default stream) and the call returns without
+ * synchronizing. The first call on a device resolves the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Every call shares the one array, so calls whose GPU work overlaps (several
+ * streams, or several host threads) race and must be serialized by the caller. */
+UNBLENDING_API int32_t unblending_unmix_device_noalloc(
+    int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
+    const unblending_options* options, const unblending_solver_options* solver,
+    double* output, int32_t* status, void* stream);
+
 /* Number of GPU kernel launches the most recent call on this thread issued. */
 UNBLENDING_API int64_t unblending_last_launch_count(void);
 

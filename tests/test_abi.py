@@ -132,6 +132,17 @@ def test_solver_option_validation(small):
             U.unmix_ex(small.image, small.layers, solver=so)
 
 
+def test_noalloc_rejects_images_beyond_its_scratch_before_any_device_work():
+    # The size limit of the allocation-free first pass (2048*2048 pixels) is
+    # checked before any CUDA call, so this runs without a GPU; the pointers
+    # are never dereferenced.
+    wl = syn.workload("rgb256_l3", 4, 4)
+    arr = syn.layer_array(wl.layers)
+    rc = U.lib.unblending_unmix_device_noalloc(2049, 2048, ctypes.c_void_p(16), arr, 3, ctypes.byref(U.options()),
+                                               ctypes.byref(U.solver_options()), ctypes.c_void_p(16), None, None)
+    assert rc == U.INVALID_ARGUMENT
+
+
 def test_too_many_layers_rejected():
     wl = syn.generate(4, 4, [0] * 9, (2.0, 3.0), seed=1)
     with pytest.raises(ValueError):

@@ -32,6 +32,7 @@ PRECISION_FP32, PRECISION_FP64 = 0, 1
 EXPORTED = [
     "unblending_abi_version", "unblending_unmix", "unblending_refine", "unblending_unmix_ex",
     "unblending_refine_ex", "unblending_unmix_device", "unblending_refine_device", "unblending_last_launch_count",
+    "unblending_unmix_device_noalloc",
 ]
 
 
@@ -80,7 +81,7 @@ def solver_options(precision=PRECISION_FP32, starts=1, radius=-1, epsilon=1e-4, 
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: run `python -m unblending_b200.build` (or __graft_entry__.build())")
+        raise ImportError(f"{LIB_PATH} is missing: run `python unblending_b200/build.py` (or __graft_entry__.build())")
     lib = ctypes.CDLL(LIB_PATH)
     P, dp = ctypes.POINTER, ctypes.POINTER(ctypes.c_double)
     lib.unblending_abi_version.restype = ctypes.c_uint32
@@ -106,6 +107,10 @@ def _load():
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              P(Stats)]
     lib.unblending_last_launch_count.restype = ctypes.c_int64
+    lib.unblending_unmix_device_noalloc.restype = ctypes.c_int32
+    lib.unblending_unmix_device_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]
     return lib
 
 
@@ -231,6 +236,17 @@ def refine_device(width, height, d_image, layers, d_first, d_output, opaque=True
                                       ctypes.byref(st) if stats else None)
     _check(rc)
     return st.as_dict() if stats else None
+
+
+def unmix_device_noalloc(width, height, d_image, layers, d_output, opaque=True, solver=None, d_status=None,
+                         stream=None):
+    """First pass that allocates no device memory (fixed scratch array of the
+    library; up to 2048*2048 pixels). For callers that cannot allocate during
+    processing. Calls that overlap on the GPU race on the shared scratch."""
+    arr, L = _layers(layers)
+    rc = lib.unblending_unmix_device_noalloc(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+                                             ctypes.byref(solver or solver_options()), d_output, d_status, stream)
+    _check(rc)
 
 
 def last_launch_count() -> int:

@@ -4,7 +4,8 @@ Each CUDA translation unit is compiled for sm_100a with nvcc; the host C++
 with g++; the shared object is linked with the exported-symbol list of
 csrc/exports.map and soname libunblending.so.1 (the reference's SDK naming,
 unblending/CMakeLists.txt:43-56). Objects are rebuilt only when a source or
-header is newer. Usage: `python -m unblending_b200.build [--force]`.
+header is newer. Usage: `python unblending_b200/build.py [--force]` (by path: importing the
+package needs the library this produces).
 """
 from __future__ import annotations
 
@@ -30,6 +31,7 @@ UNITS = [
     ("solver_fp32.cu", []),
     ("solver_fp64.cu", ["--fmad=false"]),
     ("filter.cu", ["--fmad=false"]),
+    ("noalloc.cu", []),
     ("pixels.cpp", ["-I" + os.path.join(ROOT, "include")]),
     ("unblending_c.cpp", []),
 ]

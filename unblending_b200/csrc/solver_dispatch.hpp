@@ -26,4 +26,10 @@ struct FilterArgs {
 size_t filter_scratch_doubles(int width, int height, int layers, int smooth);
 cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s);
 
+// Fixed scratch of the allocation-free first pass (noalloc.cu): device
+// address on the current device (resolved on the first call per device),
+// its size, and the largest image it serves.
+cudaError_t noalloc_scratch(void** ptr, size_t* bytes, size_t* max_pixels);
+size_t noalloc_max_pixels();   // no CUDA call
+
 }  // namespace unb

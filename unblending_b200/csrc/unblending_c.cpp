@@ -486,4 +486,70 @@ int32_t unblending_refine_device(int32_t width, int32_t height, const double* im
 
 int64_t unblending_last_launch_count(void) { return t_launches; }
 
+// First pass without any allocation: the solve's scratch (queue heads, miss
+// counters, miss lists) comes from the fixed array of noalloc.cu, and the
+// work runs on the caller's stream with no library stream or event.
+int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const double* image,
+                                        const unblending_layer* layers, size_t layer_count,
+                                        const unblending_options* options, const unblending_solver_options* solver,
+                                        double* output, int32_t* status, void* stream) {
+    t_launches = 0;
+    unblending_rgb_view view{image, 0, width, height, 0};
+    Spec sp;
+    int32_t rc = validate(&view, layers, layer_count, options, output, 0, false, nullptr, 0, sp, true);
+    if (rc != UNBLENDING_OK) return rc;
+    unblending_solver_options so;
+    if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
+    if (sp.pixels > noalloc_max_pixels()) return UNBLENDING_INVALID_ARGUMENT;   // checked before any CUDA call
+    return guarded([&]() -> int32_t {
+        void* base = nullptr;
+        size_t bytes = 0, max_pixels = 0;
+        ck(noalloc_scratch(&base, &bytes, &max_pixels));
+        if (sp.pixels > max_pixels) return UNBLENDING_INVALID_ARGUMENT;
+        int dev = 0, sms = 0;
+        ck(cudaGetDevice(&dev));
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int L = sp.layers;
+        const size_t n = sp.pixels;
+        // Layout: [0,32) queue heads, [32,64) counters, [256, ...) two lists.
+        uint32_t* queues = static_cast<uint32_t*>(base);
+        int32_t* counts = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(base) + 32);
+        int32_t* list_a = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(base) + 256);
+        int32_t* list_b = list_a + n;
+        // The array keeps the previous call's contents: the queue heads and
+        // counters must start at zero; the lists are written before they are read.
+        ck(cudaMemsetAsync(base, 0, 64, s));
+        SolverControls ctl;
+        ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
+        ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+        SolveArgs a;
+        a.n = int(n);
+        a.image = image; a.out = output; a.status = status;
+        a.opaque = sp.opaque; a.smooth = 0;
+        a.queue = queues;
+        a.miss_list = list_a;
+        a.miss_count = counts + 0;
+        const int threads = so.threads_per_block ? so.threads_per_block : 128;
+        if (so.precision == UNBLENDING_PRECISION_FP64) {
+            ck(launch_solve_fp64(L, false, make_models<double>(layers, L), ctl, a, threads, sms, s));
+            ++t_launches;
+        } else {
+            const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
+            ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl, a, threads, sms, s));
+            ++t_launches;
+            if (so.resolve_misses) {
+                SolveArgs b = a;
+                b.list = list_a; b.list_count = counts + 0;
+                b.miss_list = list_b; b.miss_count = counts + 1;
+                b.queue = queues + 1;
+                ck(launch_solve_fp64(L, false, make_models<double>(layers, L), ctl, b, threads, sms, s));
+                ++t_launches;
+            }
+        }
+        ck(cudaPeekAtLastError());
+        return UNBLENDING_OK;
+    });
+}
+
 }  // extern "C"
