@@ -38,11 +38,60 @@ typedef struct unblending_solver_options {
     double inner_tolerance;     /* default 5e-3 */
     double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
     int32_t threads_per_block;  /* 0 selects the tuned default */
-    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1 in shared memory */
+    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1/2 in shared memory
+                                   with registers capped for 4/3 blocks per SM */
+    const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL }
+
+/* Learned warm start (no counterpart in the reference). A per-pixel MLP,
+ * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the
+ * pixel's own colour) -> 64 -> 64 -> 64 (GELU) -> 4L outputs (sigmoid): the
+ * solver's start point [alpha_0..alpha_{L-1}, rgb_0..rgb_{L-1}]. BF16 weights,
+ * FP32 accumulation, tensor-core (tcgen05) training and inference kernels.
+ * Weights are out x in, row-major; unused rows of w4/b4 are zero. */
+typedef struct unblending_mlp {
+    uint32_t struct_size;
+    int32_t layer_count;        /* L the network predicts for (1..8) */
+    float w1[64 * 32], w2[64 * 64], w3[64 * 64], w4[32 * 64];
+    float b1[64], b2[64], b3[64], b4[32];
+    float loss;                 /* mean squared error of the last training batch */
+    int32_t steps;              /* Adam steps taken */
+} unblending_mlp;
+
+typedef struct unblending_mlp_options {
+    uint32_t struct_size;
+    int32_t batch;              /* samples per Adam step, default 8192 */
+    int32_t steps;              /* Adam steps, default 512 */
+    float learning_rate;        /* default 1e-3 */
+    uint64_t seed;              /* initialization and batch sampling */
+} unblending_mlp_options;
+
+#define UNBLENDING_MLP_OPTIONS_INIT { (uint32_t)sizeof(unblending_mlp_options), 8192, 512, 1e-3f, 1 }
+
+/* Trains `model` on the decompositions that this library's first pass
+ * (cold start, `solver` controls, warm_start ignored) computes for `count`
+ * device-resident images (packed RGB doubles, image k of widths[k] x
+ * heights[k]) sharing the given layers. Synchronous. */
+UNBLENDING_API int32_t unblending_mlp_train_device(
+    int32_t count, const int32_t* widths, const int32_t* heights, const double* const* images,
+    const unblending_layer* layers, size_t layer_count, const unblending_options* options,
+    const unblending_solver_options* solver, const unblending_mlp_options* mlp_options, unblending_mlp* model);
+
+/* Gradient of the training loss (mean over samples and outputs of the
+ * squared error between the sigmoid outputs and targets) of `model` on
+ * `count` samples: features (device, count x 32 floats, the last two zero)
+ * and targets (device, count x 4L floats). dL/dW and dL/db are written to the
+ * weight and bias fields of `gradient` (host), the loss to gradient->loss. */
+UNBLENDING_API int32_t unblending_mlp_loss_grad_device(
+    const unblending_mlp* model, int32_t count, const float* features, const float* targets, unblending_mlp* gradient);
+
+/* The network's start point for every pixel of a device-resident image:
+ * out is device memory of width*height*4L floats (pixel-major). */
+UNBLENDING_API int32_t unblending_mlp_predict_device(
+    const unblending_mlp* model, int32_t width, int32_t height, const double* image, float* out, void* stream);
 
 /* Per-call report. Times are device time measured with CUDA events. */
 typedef struct unblending_stats {

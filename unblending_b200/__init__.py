@@ -32,7 +32,8 @@ PRECISION_FP32, PRECISION_FP64 = 0, 1
 EXPORTED = [
     "unblending_abi_version", "unblending_unmix", "unblending_refine", "unblending_unmix_ex",
     "unblending_refine_ex", "unblending_unmix_device", "unblending_refine_device", "unblending_last_launch_count",
-    "unblending_unmix_device_noalloc",
+    "unblending_unmix_device_noalloc", "unblending_mlp_train_device", "unblending_mlp_loss_grad_device",
+    "unblending_mlp_predict_device",
 ]
 
 
@@ -55,7 +56,36 @@ class SolverOptions(ctypes.Structure):
                 ("radius", ctypes.c_int32), ("epsilon", ctypes.c_double), ("resolve_misses", ctypes.c_int32),
                 ("inner", ctypes.c_int32), ("outer", ctypes.c_int32), ("inner_tolerance", ctypes.c_double),
                 ("outer_tolerance", ctypes.c_double), ("threads_per_block", ctypes.c_int32),
-                ("kernel_variant", ctypes.c_int32)]
+                ("kernel_variant", ctypes.c_int32), ("warm_start", ctypes.c_void_p)]
+
+
+class Mlp(ctypes.Structure):
+    """ctypes mirror of `unblending_mlp` (learned warm start)."""
+    _fields_ = [("struct_size", ctypes.c_uint32), ("layer_count", ctypes.c_int32),
+                ("w1", ctypes.c_float * (64 * 32)), ("w2", ctypes.c_float * (64 * 64)),
+                ("w3", ctypes.c_float * (64 * 64)), ("w4", ctypes.c_float * (32 * 64)),
+                ("b1", ctypes.c_float * 64), ("b2", ctypes.c_float * 64), ("b3", ctypes.c_float * 64),
+                ("b4", ctypes.c_float * 32), ("loss", ctypes.c_float), ("steps", ctypes.c_int32)]
+
+    SHAPES = {"w1": (64, 32), "w2": (64, 64), "w3": (64, 64), "w4": (32, 64), "b1": (64,), "b2": (64,),
+              "b3": (64,), "b4": (32,)}
+
+    @classmethod
+    def new(cls):
+        m = cls()
+        m.struct_size = ctypes.sizeof(cls)
+        return m
+
+    def get(self, name) -> np.ndarray:
+        return np.ctypeslib.as_array(getattr(self, name)).reshape(self.SHAPES[name]).copy()
+
+    def set(self, name, value):
+        np.ctypeslib.as_array(getattr(self, name))[:] = np.asarray(value, dtype=np.float32).reshape(-1)
+
+
+class MlpOptions(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("batch", ctypes.c_int32), ("steps", ctypes.c_int32),
+                ("learning_rate", ctypes.c_float), ("seed", ctypes.c_uint64)]
 
 
 class Stats(ctypes.Structure):
@@ -74,9 +104,12 @@ def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> O
 
 def solver_options(precision=PRECISION_FP32, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
                    outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0,
-                   kernel_variant=-1) -> SolverOptions:
-    return SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
-                         outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant)
+                   kernel_variant=-1, warm_start=None) -> SolverOptions:
+    so = SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
+                       outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant,
+                       ctypes.addressof(warm_start) if warm_start is not None else None)
+    so._keep = warm_start   # the model must outlive the options
+    return so
 
 
 def _load():
@@ -107,6 +140,15 @@ def _load():
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              P(Stats)]
     lib.unblending_last_launch_count.restype = ctypes.c_int64
+    lib.unblending_mlp_train_device.restype = ctypes.c_int32
+    lib.unblending_mlp_train_device.argtypes = [ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32),
+                                                P(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_size_t, P(Options),
+                                                P(SolverOptions), P(MlpOptions), P(Mlp)]
+    lib.unblending_mlp_loss_grad_device.restype = ctypes.c_int32
+    lib.unblending_mlp_loss_grad_device.argtypes = [P(Mlp), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, P(Mlp)]
+    lib.unblending_mlp_predict_device.restype = ctypes.c_int32
+    lib.unblending_mlp_predict_device.argtypes = [P(Mlp), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p]
     lib.unblending_unmix_device_noalloc.restype = ctypes.c_int32
     lib.unblending_unmix_device_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
@@ -247,6 +289,33 @@ def unmix_device_noalloc(width, height, d_image, layers, d_output, opaque=True, 
     rc = lib.unblending_unmix_device_noalloc(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
                                              ctypes.byref(solver or solver_options()), d_output, d_status, stream)
     _check(rc)
+
+
+def mlp_train_device(images, layers, solver=None, batch=8192, steps=512, learning_rate=1e-3, seed=1,
+                     opaque=True) -> Mlp:
+    """Train the warm-start network on device images [(d_ptr, w, h), ...]
+    sharing `layers`; targets are this library's cold-start first passes."""
+    arr, L = _layers(layers)
+    k = len(images)
+    ptrs = (ctypes.c_void_p * k)(*[p for p, _, _ in images])
+    ws = (ctypes.c_int32 * k)(*[w for _, w, _ in images])
+    hs = (ctypes.c_int32 * k)(*[h for _, _, h in images])
+    mo = MlpOptions(ctypes.sizeof(MlpOptions), batch, steps, learning_rate, seed)
+    model = Mlp.new()
+    _check(lib.unblending_mlp_train_device(k, ws, hs, ptrs, arr, L, ctypes.byref(options(opaque)),
+                                           ctypes.byref(solver or solver_options()), ctypes.byref(mo),
+                                           ctypes.byref(model)))
+    return model
+
+
+def mlp_loss_grad_device(model: Mlp, count, d_features, d_targets) -> Mlp:
+    grad = Mlp.new()
+    _check(lib.unblending_mlp_loss_grad_device(ctypes.byref(model), count, d_features, d_targets, ctypes.byref(grad)))
+    return grad
+
+
+def mlp_predict_device(model: Mlp, width, height, d_image, d_out, stream=None):
+    _check(lib.unblending_mlp_predict_device(ctypes.byref(model), width, height, d_image, d_out, stream))
 
 
 def last_launch_count() -> int:

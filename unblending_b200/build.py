@@ -32,6 +32,8 @@ UNITS = [
     ("solver_fp64.cu", ["--fmad=false"]),
     ("filter.cu", ["--fmad=false"]),
     ("noalloc.cu", []),
+    ("mlp.cu", []),
+    ("mlp_data.cu", []),
     ("pixels.cpp", ["-I" + os.path.join(ROOT, "include")]),
     ("unblending_c.cpp", []),
 ]

@@ -82,6 +82,7 @@ struct SolveArgs {
     uint32_t* queue = nullptr;         // work-queue head (zeroed before launch)
     const int32_t* input_status = nullptr;  // refinement: nonzero = targets not normalizable (status 8, not solved)
     int32_t* input_failed = nullptr;        // count of such pixels
+    const float* warm = nullptr;            // optional start-0 seed: n x 4L floats, pixel-major x
     int opaque = 1, smooth = 0;
 };
 

@@ -575,6 +575,12 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
             } else {
                 init[l] = (opaque && l == 0) ? T(1) : (REFINE ? ahat[REFINE ? l : 0] : T(0.5));
             }
+            if (!REFINE && a.warm) {
+                // Learned warm start: the network's prediction replaces the
+                // start-0 seed (bounds still apply when the start is seeded).
+                const float* wv = a.warm + i * size_t(4 * L);
+                init[l] = T(colour ? wv[L + 3 * l + Q.q] : wv[l]);
+            }
         }
         have_best = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);

@@ -1,5 +1,7 @@
 // Host-side entry points of the compiled solve and filter kernels.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace unb {
@@ -31,5 +33,37 @@ cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s);
 // its size, and the largest image it serves.
 cudaError_t noalloc_scratch(void** ptr, size_t* bytes, size_t* max_pixels);
 size_t noalloc_max_pixels();   // no CUDA call
+
+// Warm-start MLP (mlp.cu): 32 -> 64 -> 64 -> 64 -> 32, BF16 weights
+// (out x in, row-major) and FP32 biases on the device.
+struct MlpDevice {
+    const __nv_bfloat16* w[4];
+    const float* b[4];
+};
+struct MlpGrad {
+    float* w[4];
+    float* b[4];
+    float* loss;
+};
+struct MlpMaster {
+    float* w[4];
+    float* b[4];
+    float* mw[4];
+    float* vw[4];
+    float* mb[4];
+    float* vb[4];
+};
+constexpr int kMlpIn = 32, kMlpHidden = 64, kMlpOut = 32;
+cudaError_t launch_mlp_infer(const MlpDevice& p, const double* image, int w, int h, int L, float* out,
+                             int32_t* error, int sms, cudaStream_t s);
+cudaError_t launch_mlp_features(const double* image, int w, int h, float* feats, cudaStream_t s);
+cudaError_t launch_mlp_train(const MlpDevice& p, const float* feats, const float* targets, int count, int outs,
+                             const MlpGrad& g, int32_t* error, int sms, cudaStream_t s);
+cudaError_t launch_mlp_adam(const MlpMaster& m, const MlpGrad& g, const MlpDevice& p, float lr, int step,
+                            cudaStream_t s);
+// Training batch assembly and targets (mlp_data.cu).
+cudaError_t launch_gather_targets(const double* packed, int64_t n, int L, float* targets, cudaStream_t s);
+cudaError_t launch_sample_batch(const float* feats, const float* targets, int64_t pool, int outs, int batch,
+                                uint64_t seed, float* bfeats, float* btargets, cudaStream_t s);
 
 }  // namespace unb

@@ -1,32 +1,33 @@
 // FP32 instantiations of the per-pixel solve. Variant 0 keeps the L-BFGS
-// history in registers (fewer, fatter warps); variant 1 keeps it in shared
-// memory and caps registers for four 128-thread blocks per SM.
+// history in registers (fewer, fatter warps); variants 1 and 2 keep it in
+// shared memory and cap registers for four (1) or three (2) 128-thread
+// blocks per SM.
 #include "solver_dispatch.hpp"
 #include "solver_kernels.cuh"
 
 namespace unb {
 
 namespace {
-template <int L, bool R, bool H> cudaError_t go(const Models<float>& m, const SolverControls& c, const SolveArgs& a,
+template <int L, bool R, bool H, int B> cudaError_t go(const Models<float>& m, const SolverControls& c, const SolveArgs& a,
                                                 int threads, int sms, cudaStream_t s) {
-    using Launch = SolveLauncher<float, L, R, H>;
+    using Launch = SolveLauncher<float, L, R, H, B>;
     int per_sm = 0;
     cudaError_t e = Launch::occupancy(threads, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     return Launch::launch(m, c, a, per_sm * sms, threads, s);
 }
-template <bool R, bool H> cudaError_t pick(int L, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
+template <bool R, bool H, int B> cudaError_t pick(int L, const Models<float>& m, const SolverControls& c, const SolveArgs& a,
                                            int threads, int sms, cudaStream_t s) {
     switch (L) {
-    case 1: return go<1, R, H>(m, c, a, threads, sms, s);
-    case 2: return go<2, R, H>(m, c, a, threads, sms, s);
-    case 3: return go<3, R, H>(m, c, a, threads, sms, s);
-    case 4: return go<4, R, H>(m, c, a, threads, sms, s);
-    case 5: return go<5, R, H>(m, c, a, threads, sms, s);
-    case 6: return go<6, R, H>(m, c, a, threads, sms, s);
-    case 7: return go<7, R, H>(m, c, a, threads, sms, s);
-    case 8: return go<8, R, H>(m, c, a, threads, sms, s);
+    case 1: return go<1, R, H, B>(m, c, a, threads, sms, s);
+    case 2: return go<2, R, H, B>(m, c, a, threads, sms, s);
+    case 3: return go<3, R, H, B>(m, c, a, threads, sms, s);
+    case 4: return go<4, R, H, B>(m, c, a, threads, sms, s);
+    case 5: return go<5, R, H, B>(m, c, a, threads, sms, s);
+    case 6: return go<6, R, H, B>(m, c, a, threads, sms, s);
+    case 7: return go<7, R, H, B>(m, c, a, threads, sms, s);
+    case 8: return go<8, R, H, B>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -35,8 +36,10 @@ template <bool R, bool H> cudaError_t pick(int L, const Models<float>& m, const 
 cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<float>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s) {
     if (variant == 1)
-        return refine ? pick<true, true>(L, m, c, a, threads, sms, s) : pick<false, true>(L, m, c, a, threads, sms, s);
-    return refine ? pick<true, false>(L, m, c, a, threads, sms, s) : pick<false, false>(L, m, c, a, threads, sms, s);
+        return refine ? pick<true, true, 4>(L, m, c, a, threads, sms, s) : pick<false, true, 4>(L, m, c, a, threads, sms, s);
+    if (variant == 2)
+        return refine ? pick<true, true, 3>(L, m, c, a, threads, sms, s) : pick<false, true, 3>(L, m, c, a, threads, sms, s);
+    return refine ? pick<true, false, 1>(L, m, c, a, threads, sms, s) : pick<false, false, 1>(L, m, c, a, threads, sms, s);
 }
 
 }  // namespace unb

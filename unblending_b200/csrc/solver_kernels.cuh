@@ -6,8 +6,9 @@
 
 namespace unb {
 
-template <class T, int L, bool REFINE, bool HSMEM>
-__global__ void __launch_bounds__(128, (HSMEM && sizeof(T) == 4) ? 4 : 1)
+// MINB: blocks per SM the register allocation must allow (launch bounds).
+template <class T, int L, bool REFINE, bool HSMEM, int MINB>
+__global__ void __launch_bounds__(128, MINB)
 solve_pixels(const __grid_constant__ Models<T> m, const __grid_constant__ SolverControls ctl,
              const __grid_constant__ SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -16,11 +17,11 @@ solve_pixels(const __grid_constant__ Models<T> m, const __grid_constant__ Solver
     S.run();
 }
 
-template <class T, int L, bool REFINE, bool HSMEM> struct SolveLauncher {
+template <class T, int L, bool REFINE, bool HSMEM, int MINB = 1> struct SolveLauncher {
     static size_t smem_bytes(int threads) { return HSMEM ? size_t(threads) * kHistory * L * 2 * sizeof(T) : 0; }
 
     static cudaError_t occupancy(int threads, int* blocks_per_sm) {
-        auto k = solve_pixels<T, L, REFINE, HSMEM>;
+        auto k = solve_pixels<T, L, REFINE, HSMEM, MINB>;
         const size_t sm = smem_bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
@@ -31,7 +32,7 @@ template <class T, int L, bool REFINE, bool HSMEM> struct SolveLauncher {
 
     static cudaError_t launch(const Models<T>& m, const SolverControls& ctl, const SolveArgs& a, int blocks,
                               int threads, cudaStream_t stream) {
-        auto k = solve_pixels<T, L, REFINE, HSMEM>;
+        auto k = solve_pixels<T, L, REFINE, HSMEM, MINB>;
         const size_t sm = smem_bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));

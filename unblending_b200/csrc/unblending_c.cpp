@@ -44,6 +44,10 @@ thread_local int64_t t_launches = 0;
 struct Buffer {
     void* ptr = nullptr;
     size_t bytes = 0;
+    Buffer() = default;
+    Buffer(const Buffer&) = delete;
+    Buffer& operator=(const Buffer&) = delete;
+    ~Buffer() { if (ptr) cudaFree(ptr); }
     template <class T> T* get(size_t count) {
         const size_t want = std::max<size_t>(count * sizeof(T), 256);
         if (want > bytes) {
@@ -64,6 +68,8 @@ struct Context {
     cudaEvent_t ev[6] = {};
     std::mutex mutex;
     Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters;
+    Buffer warm, mlp_w, mlp_b;               // warm-start network on the device
+    std::vector<float> mlp_uploaded;         // parameters currently in mlp_w / mlp_b
     explicit Context(int dev) : device(dev) {
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -190,7 +196,7 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
         (out.resolve_misses != 0 && out.resolve_misses != 1) ||
         (out.threads_per_block != 0 && (out.threads_per_block % 32 != 0 || out.threads_per_block < 32 ||
                                         out.threads_per_block > 128)) ||
-        out.kernel_variant < -1 || out.kernel_variant > 1)
+        out.kernel_variant < -1 || out.kernel_variant > 2)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -213,6 +219,58 @@ template <class T> Models<T> make_models(const unblending_layer* layers, int L) 
         set_blend_table(m, l, layers[l].blend_mode);
     }
     return m;
+}
+
+// ------------------------------------------------------- warm-start MLP --
+constexpr int kMlpSizes[4][2] = {{kMlpHidden, kMlpIn}, {kMlpHidden, kMlpHidden}, {kMlpHidden, kMlpHidden},
+                                 {kMlpOut, kMlpHidden}};
+
+const float* mlp_weight(const unblending_mlp& m, int k) { return k == 0 ? m.w1 : k == 1 ? m.w2 : k == 2 ? m.w3 : m.w4; }
+const float* mlp_bias(const unblending_mlp& m, int k) { return k == 0 ? m.b1 : k == 1 ? m.b2 : k == 2 ? m.b3 : m.b4; }
+float* mlp_weight(unblending_mlp& m, int k) { return k == 0 ? m.w1 : k == 1 ? m.w2 : k == 2 ? m.w3 : m.w4; }
+float* mlp_bias(unblending_mlp& m, int k) { return k == 0 ? m.b1 : k == 1 ? m.b2 : k == 2 ? m.b3 : m.b4; }
+
+size_t mlp_weight_count() {
+    size_t s = 0;
+    for (auto& d : kMlpSizes) s += size_t(d[0]) * d[1];
+    return s;
+}
+size_t mlp_bias_count() { return 3 * kMlpHidden + kMlpOut; }
+
+bool mlp_valid(const unblending_mlp* m, int L) {
+    if (!m || m->struct_size < sizeof(unblending_mlp) || m->layer_count != L) return false;
+    for (int k = 0; k < 4; ++k) {
+        for (int i = 0; i < kMlpSizes[k][0] * kMlpSizes[k][1]; ++i) if (!std::isfinite(mlp_weight(*m, k)[i])) return false;
+        for (int i = 0; i < kMlpSizes[k][0]; ++i) if (!std::isfinite(mlp_bias(*m, k)[i])) return false;
+    }
+    return true;
+}
+
+// Device copy of a network (BF16 weights, FP32 biases), uploaded when it
+// differs from the one already on this device.
+MlpDevice upload_model(Context& c, const unblending_mlp& m, cudaStream_t s) {
+    __nv_bfloat16* w = c.mlp_w.get<__nv_bfloat16>(mlp_weight_count());
+    float* b = c.mlp_b.get<float>(mlp_bias_count());
+    std::vector<float> flat;
+    flat.reserve(mlp_weight_count() + mlp_bias_count());
+    for (int k = 0; k < 4; ++k) flat.insert(flat.end(), mlp_weight(m, k), mlp_weight(m, k) + kMlpSizes[k][0] * kMlpSizes[k][1]);
+    for (int k = 0; k < 4; ++k) flat.insert(flat.end(), mlp_bias(m, k), mlp_bias(m, k) + kMlpSizes[k][0]);
+    if (flat != c.mlp_uploaded) {
+        std::vector<__nv_bfloat16> wb(mlp_weight_count());
+        for (size_t i = 0; i < wb.size(); ++i) wb[i] = __float2bfloat16(flat[i]);
+        ck(cudaMemcpyAsync(w, wb.data(), wb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, s));
+        ck(cudaMemcpyAsync(b, flat.data() + mlp_weight_count(), mlp_bias_count() * sizeof(float),
+                           cudaMemcpyHostToDevice, s));
+        ck(cudaStreamSynchronize(s));   // host staging vectors go out of scope
+        c.mlp_uploaded = std::move(flat);
+    }
+    MlpDevice d;
+    size_t off = 0, boff = 0;
+    for (int k = 0; k < 4; ++k) {
+        d.w[k] = w + off; off += size_t(kMlpSizes[k][0]) * kMlpSizes[k][1];
+        d.b[k] = b + boff; boff += kMlpSizes[k][0];
+    }
+    return d;
 }
 
 // --------------------------------------------------------------- a pass --
@@ -270,6 +328,14 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     a.queue = queues;
     a.miss_list = c.list_a.get<int32_t>(n);
     a.miss_count = counts + 0;
+    if (!refine && so.warm_start) {
+        // Learned start point for every pixel, then the solve from it.
+        const MlpDevice dev = upload_model(c, *so.warm_start, s);
+        float* warm = c.warm.get<float>(size_t(4) * L * n);
+        ck(launch_mlp_infer(dev, io.image, sp.width, sp.height, L, warm, counts + 3, c.sms, s));
+        ++t_launches;
+        a.warm = warm;
+    }
     const int threads = so.threads_per_block ? so.threads_per_block : 128;
     if (so.precision == UNBLENDING_PRECISION_FP64) {
         ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, a, threads, c.sms, s));
@@ -288,6 +354,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
             b.miss_count = counts + 1;
             b.queue = queues + 1;
             b.input_status = nullptr; b.input_failed = nullptr;
+            b.warm = nullptr;   // misses fall back to the reference's (cold) start
             ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, b, threads, c.sms, s));
             ++t_launches;
         } else {
@@ -327,6 +394,8 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
     unblending_solver_options so;
     if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
     if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
+    if (refine) so.warm_start = nullptr;   // the learned start seeds the first pass only
+    if (so.warm_start && !mlp_valid(so.warm_start, sp.layers)) return UNBLENDING_INVALID_ARGUMENT;
     return guarded([&]() -> int32_t {
         Context& c = context();
         std::lock_guard<std::mutex> lock(c.mutex);
@@ -394,6 +463,8 @@ int32_t device_call(int32_t width, int32_t height, const double* image, const un
     unblending_solver_options so;
     if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
     if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
+    if (refine) so.warm_start = nullptr;   // the learned start seeds the first pass only
+    if (so.warm_start && !mlp_valid(so.warm_start, sp.layers)) return UNBLENDING_INVALID_ARGUMENT;
     return guarded([&]() -> int32_t {
         Context& c = context();
         std::lock_guard<std::mutex> lock(c.mutex);
@@ -485,6 +556,213 @@ int32_t unblending_refine_device(int32_t width, int32_t height, const double* im
 }
 
 int64_t unblending_last_launch_count(void) { return t_launches; }
+
+int32_t unblending_mlp_predict_device(const unblending_mlp* model, int32_t width, int32_t height, const double* image,
+                                      float* out, void* stream) {
+    t_launches = 0;
+    if (!model || !image || !out || width <= 0 || height <= 0 || width > std::numeric_limits<int>::max() / height)
+        return UNBLENDING_INVALID_ARGUMENT;
+    if (model->layer_count < 1 || model->layer_count > kMaxLayers || !mlp_valid(model, model->layer_count))
+        return UNBLENDING_INVALID_ARGUMENT;
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+        const MlpDevice dev = upload_model(c, *model, s);
+        int32_t* err = c.small.get<int32_t>(8) + 7;
+        ck(cudaMemsetAsync(err, 0, sizeof(int32_t), s));
+        ck(launch_mlp_infer(dev, image, width, height, model->layer_count, out, err, c.sms, s));
+        ++t_launches;
+        int32_t failed = 0;
+        ck(cudaMemcpyAsync(&failed, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        ck(cudaStreamSynchronize(s));
+        if (failed) throw CudaFailure(cudaErrorLaunchTimeout);
+        return UNBLENDING_OK;
+    });
+}
+
+int32_t unblending_mlp_loss_grad_device(const unblending_mlp* model, int32_t count, const float* features,
+                                        const float* targets, unblending_mlp* gradient) {
+    t_launches = 0;
+    if (!model || !features || !targets || !gradient || count < 1 || gradient->struct_size < sizeof(unblending_mlp))
+        return UNBLENDING_INVALID_ARGUMENT;
+    if (model->layer_count < 1 || model->layer_count > kMaxLayers || !mlp_valid(model, model->layer_count))
+        return UNBLENDING_INVALID_ARGUMENT;
+    const int outs = 4 * model->layer_count;
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = c.stream;
+        const MlpDevice dev = upload_model(c, *model, s);
+        const size_t nw = mlp_weight_count(), nb = mlp_bias_count(), np = nw + nb;
+        Buffer grad_b;
+        float* grad = grad_b.get<float>(np + 1);
+        ck(cudaMemsetAsync(grad, 0, (np + 1) * sizeof(float), s));
+        MlpGrad g;
+        size_t o = 0, ob = nw;
+        for (int k = 0; k < 4; ++k) {
+            g.w[k] = grad + o; o += size_t(kMlpSizes[k][0]) * kMlpSizes[k][1];
+            g.b[k] = grad + ob; ob += kMlpSizes[k][0];
+        }
+        g.loss = grad + np;
+        int32_t* err = c.small.get<int32_t>(8) + 7;
+        ck(cudaMemsetAsync(err, 0, sizeof(int32_t), s));
+        ck(launch_mlp_train(dev, features, targets, count, outs, g, err, c.sms, s));
+        ++t_launches;
+        std::vector<float> out(np + 1);
+        int32_t failed = 0;
+        ck(cudaMemcpyAsync(out.data(), grad, (np + 1) * sizeof(float), cudaMemcpyDeviceToHost, s));
+        ck(cudaMemcpyAsync(&failed, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        ck(cudaStreamSynchronize(s));
+        if (failed) throw CudaFailure(cudaErrorLaunchTimeout);
+        gradient->layer_count = model->layer_count;
+        o = 0;
+        for (int k = 0; k < 4; ++k) {
+            const size_t sz = size_t(kMlpSizes[k][0]) * kMlpSizes[k][1];
+            std::copy(out.begin() + o, out.begin() + o + sz, mlp_weight(*gradient, k));
+            o += sz;
+        }
+        for (int k = 0; k < 4; ++k) {
+            std::copy(out.begin() + o, out.begin() + o + kMlpSizes[k][0], mlp_bias(*gradient, k));
+            o += kMlpSizes[k][0];
+        }
+        gradient->loss = out[np] / float(size_t(count) * outs);
+        gradient->steps = 0;
+        return UNBLENDING_OK;
+    });
+}
+
+int32_t unblending_mlp_train_device(int32_t count, const int32_t* widths, const int32_t* heights,
+                                    const double* const* images, const unblending_layer* layers, size_t layer_count,
+                                    const unblending_options* options, const unblending_solver_options* solver,
+                                    const unblending_mlp_options* mlp_options, unblending_mlp* model) {
+    t_launches = 0;
+    if (count <= 0 || !widths || !heights || !images || !model || model->struct_size < sizeof(unblending_mlp))
+        return UNBLENDING_INVALID_ARGUMENT;
+    const unblending_mlp_options mdef = UNBLENDING_MLP_OPTIONS_INIT;
+    const unblending_mlp_options mo = mlp_options ? *mlp_options : mdef;
+    if ((mlp_options && mlp_options->struct_size < sizeof(unblending_mlp_options)) || mo.batch < 128 ||
+        mo.batch > (1 << 20) || mo.steps < 1 || !(mo.learning_rate > 0))
+        return UNBLENDING_INVALID_ARGUMENT;
+    unblending_solver_options so;
+    int32_t rc = resolve_solver(solver, so);
+    if (rc != UNBLENDING_OK) return rc;
+    so.warm_start = nullptr;   // targets come from the reference's start
+    std::vector<Spec> specs(count);
+    size_t pool = 0, largest = 0;
+    for (int k = 0; k < count; ++k) {
+        unblending_rgb_view view{images[k], 0, widths[k], heights[k], 0};
+        rc = validate(&view, layers, layer_count, options, images[k], 0, false, nullptr, 0, specs[k], true);
+        if (rc != UNBLENDING_OK) return rc;
+        pool += specs[k].pixels;
+        largest = std::max(largest, specs[k].pixels);
+    }
+    const int L = int(layer_count), outs = 4 * L;
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = c.stream;
+        // Pool of (features, targets): the first pass of every image.
+        Buffer feats_b, targets_b, packed_b, bf_b, bt_b, master_b, grad_b, wdev_b;
+        float* feats = feats_b.get<float>(pool * kMlpIn);
+        float* targets = targets_b.get<float>(pool * outs);
+        double* packed = packed_b.get<double>(largest * outs);
+        size_t off = 0;
+        for (int k = 0; k < count; ++k) {
+            const Spec& sp = specs[k];
+            ck(launch_mlp_features(images[k], sp.width, sp.height, feats + off * kMlpIn, s));
+            PassIO io;
+            io.image = images[k];
+            io.out = packed;
+            io.status = c.status.get<int32_t>(sp.pixels);
+            enqueue_pass(c, sp, false, layers, so, io, s);
+            ck(launch_gather_targets(packed, int64_t(sp.pixels), L, targets + off * outs, s));
+            off += sp.pixels;
+        }
+        // Parameters: FP32 masters + Adam moments, BF16 copies, gradients.
+        const size_t nw = mlp_weight_count(), nb = mlp_bias_count(), np = nw + nb;
+        float* master = master_b.get<float>(3 * np);   // params | m | v
+        float* grad = grad_b.get<float>(np + 1);       // dW | db | loss
+        __nv_bfloat16* wdev = wdev_b.get<__nv_bfloat16>(nw);
+        std::vector<float> init(3 * np, 0.0f);
+        {
+            // He-uniform for the GELU layers, Glorot-uniform for the output;
+            // rows of the output layer beyond 4L stay zero.
+            uint64_t st = mo.seed * 0x9E3779B97F4A7C15ull + 1;
+            auto uni = [&]() {
+                st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+                return double(st >> 11) * (1.0 / 9007199254740992.0);
+            };
+            size_t o = 0;
+            for (int k = 0; k < 4; ++k) {
+                const int rows = kMlpSizes[k][0], cols = kMlpSizes[k][1];
+                const int fan_in = k == 0 ? 30 : cols;
+                const double bound = k < 3 ? std::sqrt(6.0 / fan_in) : std::sqrt(6.0 / (fan_in + outs));
+                for (int r = 0; r < rows; ++r)
+                    for (int q = 0; q < cols; ++q)
+                        init[o + size_t(r) * cols + q] = (k == 3 && r >= outs) ? 0.0f : float((2 * uni() - 1) * bound);
+                o += size_t(rows) * cols;
+            }
+        }
+        std::vector<__nv_bfloat16> wb(nw);
+        for (size_t i = 0; i < nw; ++i) wb[i] = __float2bfloat16(init[i]);
+        ck(cudaMemcpyAsync(master, init.data(), init.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+        ck(cudaMemcpyAsync(wdev, wb.data(), nw * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, s));
+        ck(cudaMemsetAsync(grad, 0, (np + 1) * sizeof(float), s));
+        MlpDevice dev;
+        MlpMaster mm;
+        MlpGrad g;
+        {
+            size_t o = 0, ob = nw;
+            for (int k = 0; k < 4; ++k) {
+                const size_t sz = size_t(kMlpSizes[k][0]) * kMlpSizes[k][1];
+                dev.w[k] = wdev + o;
+                mm.w[k] = master + o; mm.mw[k] = master + np + o; mm.vw[k] = master + 2 * np + o;
+                g.w[k] = grad + o;
+                o += sz;
+                dev.b[k] = master + ob;
+                mm.b[k] = master + ob; mm.mb[k] = master + np + ob; mm.vb[k] = master + 2 * np + ob;
+                g.b[k] = grad + ob;
+                ob += kMlpSizes[k][0];
+            }
+            g.loss = grad + np;
+        }
+        float* bfeats = bf_b.get<float>(size_t(mo.batch) * kMlpIn);
+        float* btargets = bt_b.get<float>(size_t(mo.batch) * outs);
+        int32_t* err = c.small.get<int32_t>(8) + 7;
+        ck(cudaMemsetAsync(err, 0, sizeof(int32_t), s));
+        float loss = 0.0f;
+        for (int step = 1; step <= mo.steps; ++step) {
+            ck(launch_sample_batch(feats, targets, int64_t(pool), outs, mo.batch, mo.seed * 1000003ull + step, bfeats,
+                                   btargets, s));
+            if (step == mo.steps) ck(cudaMemsetAsync(g.loss, 0, sizeof(float), s));
+            ck(launch_mlp_train(dev, bfeats, btargets, mo.batch, outs, g, err, c.sms, s));
+            if (step == mo.steps) ck(cudaMemcpyAsync(&loss, g.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+            ck(launch_mlp_adam(mm, g, dev, mo.learning_rate, step, s));
+            t_launches += 3;
+        }
+        std::vector<float> out(np);
+        int32_t failed = 0;
+        ck(cudaMemcpyAsync(out.data(), master, np * sizeof(float), cudaMemcpyDeviceToHost, s));
+        ck(cudaMemcpyAsync(&failed, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        ck(cudaStreamSynchronize(s));
+        if (failed) throw CudaFailure(cudaErrorLaunchTimeout);
+        model->layer_count = L;
+        size_t o = 0;
+        for (int k = 0; k < 4; ++k) {
+            const size_t sz = size_t(kMlpSizes[k][0]) * kMlpSizes[k][1];
+            std::copy(out.begin() + o, out.begin() + o + sz, mlp_weight(*model, k));
+            o += sz;
+        }
+        for (int k = 0; k < 4; ++k) {
+            std::copy(out.begin() + o, out.begin() + o + kMlpSizes[k][0], mlp_bias(*model, k));
+            o += kMlpSizes[k][0];
+        }
+        model->loss = loss / float(size_t(mo.batch) * outs);
+        model->steps = mo.steps;
+        return UNBLENDING_OK;
+    });
+}
 
 // First pass without any allocation: the solve's scratch (queue heads, miss
 // counters, miss lists) comes from the fixed array of noalloc.cu, and the

@@ -174,9 +174,15 @@ class Workload:
 
 
 def generate(width: int, height: int, modes: list[int], sigma: tuple[float, float], seed: int,
-             noise: float = 0.0, radius: int | None = None, name: str = "custom", comp=SOURCE_OVER) -> Workload:
+             noise: float = 0.0, radius: int | None = None, name: str = "custom", comp=SOURCE_OVER,
+             layers: list[LayerSpec] | None = None) -> Workload:
+    """One image. `layers` reuses given layer models (same layer infos,
+    new colours and alpha fields drawn from `seed`)."""
     rng = np.random.default_rng(seed)
-    layers = make_layers(rng, modes, comp)
+    if layers is None:
+        layers = make_layers(rng, modes, comp)
+    else:
+        rng = np.random.default_rng([seed, 7919])
     L, n = len(layers), width * height
     colors = np.empty((L, n, 3))
     alphas = np.empty((L, n))
