@@ -1,24 +1,29 @@
 """Benchmark: full decomposition (first pass + matte refinement) throughput.
 
 Workload (one step): the 1024x1024, 5-layer synthetic image (normal,
-multiply, screen, overlay, color-dodge; alpha blobs 20-200 px; seed 2),
+multiply, screen, overlay, color-dodge; alpha blobs 20-200 px; seed 2 + rank),
 colour unmixing then matte refinement with an opaque, smoothed background
 (the reference CLI's configuration, unblending-cli/main.cpp:58-66) and the
 reference's refinement radius 60*min(w,h)/1000 = 61.
 
-  value : pixels/s with the image resident in HBM (device entry points),
-          per-step device time from CUDA events on the library's stream;
-          a 256 MiB buffer is written between steps (L2 flush, untimed).
-  e2e   : the same through the C ABI calls unblending_unmix +
-          unblending_refine with pinned host buffers (uploads, the first
-          pass's round trip through the host, and downloads are timed).
+  value      : pixels/s of the plain (reference-start) FP32 solve with its
+               FP64 check and FP64 re-solve of misses, image resident in HBM,
+               per-step device time from CUDA events; a 256 MiB buffer is
+               written between steps (L2 flush, untimed).
+  warm_start : the same with the learned start on the first pass (network
+               trained beforehand on 64 seeded 256x256 images of the same layer
+               set, 2^22 pixels, batch 8192, Adam lr 1e-3).
+  fp64       : the same with the FP64 solve (replays the reference's FP64
+               solver).
+  e2e        : the plain configuration through the C ABI calls
+               unblending_unmix + unblending_refine with pinned host buffers.
 
 Multi-GPU: one process per GPU, each decomposing its own image (weak
 scaling, no collective on the data path); time = max over ranks.
 
 `--impl reference` times the reference's own CPU implementation
-(oracle/_ref, the reference's FP64 solver and CPU guided filter compiled
-from its sources; else the CPU oracle restatement) on all host cores.
+(oracle/_ref: the reference's FP64 solver and CPU guided filter compiled from
+its sources; else the CPU oracle restatement) on all host cores.
 """
 from __future__ import annotations
 
@@ -50,17 +55,11 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     p.add_argument("--width", type=int, default=1024)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-warm", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
     return p.parse_args()
-
-
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
 
 
 # ---------------------------------------------------------------- clocks --
@@ -77,8 +76,7 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self.proc = None
 
@@ -94,8 +92,9 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace('.', '', 1).isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace('.', '', 1).isdigit()]
+        num = lambda v: v.replace('.', '', 1).isdigit()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and num(r[1])]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and num(r[2])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -104,11 +103,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------ flop count --
 def evaluation_flops(L: int, modes: list[int]) -> tuple[float, float]:
-    """FP32 flops of one value evaluation and of one value+gradient evaluation
-    of the per-pixel objective, counted from the solver's arithmetic per
-    pixel (all four lanes of a quad): composite 3 channels x (L-1) layers,
-    Gaussian prior 3x3 per layer, AL terms; the gradient adds the (P+P^T)
-    rows and the reverse sweep. add/mul = 1, fma = 2, div/sqrt = 1."""
+    """FP32 flops of one value evaluation and of one value+gradient
+    evaluation of the per-pixel objective (all four lanes of a quad):
+    composite 3 channels x (L-1) layers, 3x3 Gaussian prior per layer, AL
+    rows; the gradient adds the (P+P^T) rows and the reverse sweep.
+    add/mul = 1, fma = 2, reciprocal/sqrt = 1."""
     blend_v = {0: 0, 1: 1, 2: 3, 3: 4, 4: 1, 5: 1, 6: 3, 7: 4, 8: 4, 9: 8, 10: 1, 11: 4, 12: 1}
     blend_g = {0: 0, 1: 1, 2: 5, 3: 6, 4: 1, 5: 1, 6: 7, 7: 8, 8: 6, 9: 14, 10: 1, 11: 8, 12: 1}
     val = 0.0
@@ -126,11 +125,12 @@ def evaluation_flops(L: int, modes: list[int]) -> tuple[float, float]:
 
 
 # ------------------------------------------------------------ reference --
-def cpu_reference(wl, first_gpu, final_gpu, threads, sample_idx):
+def cpu_reference(wl, first_gpu, finals, threads, sample_idx):
     """The reference's CPU implementation on this host: its FP64 solver
     (general::Optimizer<double>) for both passes over a pixel sample, and its
     CPU guided filter (general::StreamingFilterCPU) over the whole image.
-    Returns (seconds per full image extrapolated, details, parity dict)."""
+    Returns (seconds per full image, kind, details, parity of each GPU output
+    in `finals` (name -> (first, final)) on the sample)."""
     import oracle
     from unblending_b200 import synthetic as syn
     from tests.parity import report
@@ -144,12 +144,11 @@ def cpu_reference(wl, first_gpu, final_gpu, threads, sample_idx):
     t0 = time.perf_counter()
     x1, _ = impl.solve(layers, oracle.problem(L, False, True), oracle.options(), target, init, threads=threads)
     t_unmix = time.perf_counter() - t0
-    # Filter over the whole image from the GPU first pass (same input for both).
     rgb_planar = wl.image.reshape(n, 3).T.copy()
     first_x = oracle.unpack(first_gpu, L)
     first_planar = first_x.T.copy()
-    t0 = time.perf_counter()
     radius = syn.reference_radius(w, h)
+    t0 = time.perf_counter()
     if kind == "reference":
         targets = np.zeros((L + 3, n))
         status = np.zeros(n, np.int32)
@@ -171,23 +170,26 @@ def cpu_reference(wl, first_gpu, final_gpu, threads, sample_idx):
     t_refine = time.perf_counter() - t0
     x2[:, :L] = alpha
     x2[:, L:L + 3] = bg
-    per_px = (t_unmix + t_refine) / len(sample_idx)
-    seconds = t_filter + per_px * n
-    # Parity of the GPU outputs on the sample pixels.
-    gpu1 = oracle.unpack(first_gpu, L)[sample_idx]
-    gpu2 = oracle.unpack(final_gpu, L)[sample_idx]
-    par1 = report(oracle.pack(gpu1, L, len(sample_idx), 1), oracle.pack(x1, L, len(sample_idx), 1), wl.layers, False)
-    par2 = report(oracle.pack(gpu2, L, len(sample_idx), 1), oracle.pack(x2, L, len(sample_idx), 1), wl.layers, True)
+    seconds = t_filter + (t_unmix + t_refine) / len(sample_idx) * n
+    m = len(sample_idx)
+    ref1 = oracle.pack(x1, L, m, 1)
+    ref2 = oracle.pack(x2, L, m, 1)
+    parity = {}
+    for name, (first, final) in finals.items():
+        g1 = oracle.pack(oracle.unpack(first, L)[sample_idx], L, m, 1)
+        g2 = oracle.pack(oracle.unpack(final, L)[sample_idx], L, m, 1)
+        parity[name] = {"first_pass": report(g1, ref1, wl.layers, False),
+                        "refinement_same_first_pass": report(g2, ref2, wl.layers, True) if name == "plain" else None}
     details = {"t_unmix_sample_s": t_unmix, "t_refine_sample_s": t_refine, "t_filter_full_s": t_filter}
-    return seconds, kind, details, {"first_pass": par1, "refinement": par2}
+    return seconds, kind, details, parity
 
 
 def reference_arm(args):
-    rank, world, _ = dist_env()
+    from unblending_b200 import dist, synthetic as syn
+    import oracle
+    rank, world, _ = dist.env()
     if rank != 0:
         return
-    from unblending_b200 import synthetic as syn
-    import oracle
     wl = syn.workload(WORKLOAD, args.width, args.width)
     L, n = len(wl.layers), wl.pixels
     threads = os.cpu_count() or 1
@@ -197,8 +199,6 @@ def reference_arm(args):
     rng = np.random.default_rng(0)
     sample = np.sort(rng.choice(n, size=SAMPLE, replace=False))
     layers = syn.layer_array(wl.layers)
-    # The reference's first pass over the whole image (needed for its filter) is
-    # too slow for every step; steps time: full filter + solves on the sample.
     x_first_sample, _ = impl.solve(layers, oracle.problem(L, False, True), oracle.options(),
                                    wl.image.reshape(n, 3)[sample],
                                    np.tile(oracle.initial_first(wl.layers, True), (SAMPLE, 1)), threads=threads)
@@ -207,7 +207,7 @@ def reference_arm(args):
     first_packed = oracle.pack(first_full, L, wl.width, wl.height)
     times = []
     for step in range(args.warmup + args.steps):
-        seconds, kind, details, _ = cpu_reference(wl, first_packed, first_packed, threads, sample)
+        seconds, kind, details, _ = cpu_reference(wl, first_packed, {}, threads, sample)
         if step >= args.warmup:
             times.append(seconds)
     sec = float(np.mean(times))
@@ -216,7 +216,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
-        "config": {"workload": f"{WORKLOAD} {args.width}x{args.width} L=5 unmix+refine(smooth, r=ref formula)",
+        "config": {"workload": f"{WORKLOAD} {args.width}x{args.width} L=5 unmix+refine(opaque, smooth bg, r=ref formula)",
                    "warm_start": False},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"per step: CPU guided filter over the full image + both solves on {SAMPLE} "
@@ -227,13 +227,82 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ b200 --
+class Decomposition:
+    """Device buffers and the two device calls of one decomposition step."""
+
+    def __init__(self, U, torch, wl, stream):
+        self.U, self.torch, self.wl, self.stream = U, torch, wl, stream
+        L, n = len(wl.layers), wl.pixels
+        self.d_img = torch.from_numpy(wl.image.reshape(-1)).cuda()
+        self.d_first = torch.empty(4 * L * n, dtype=torch.float64, device="cuda")
+        self.d_out = torch.empty_like(self.d_first)
+        self.d_status = torch.empty(n, dtype=torch.int32, device="cuda")
+        self.c1 = torch.zeros((n, 5), dtype=torch.int32, device="cuda")
+        self.c2 = torch.zeros((n, 5), dtype=torch.int32, device="cuda")
+
+    def step(self, solver, counters=False, stats=False):
+        U, wl = self.U, self.wl
+        s1 = U.unmix_device(wl.width, wl.height, self.d_img.data_ptr(), wl.layers, self.d_first.data_ptr(),
+                            solver=solver, d_status=self.d_status.data_ptr(),
+                            d_counters=self.c1.data_ptr() if counters else None, stream=self.stream, stats=stats)
+        k = U.last_launch_count()
+        s2 = U.refine_device(wl.width, wl.height, self.d_img.data_ptr(), wl.layers, self.d_first.data_ptr(),
+                             self.d_out.data_ptr(), smooth=True, solver=solver, d_status=self.d_status.data_ptr(),
+                             d_counters=self.c2.data_ptr() if counters else None, stream=self.stream, stats=stats)
+        return s1, s2, k + U.last_launch_count()
+
+    def timed(self, solver, steps, warmup, flush):
+        torch = self.torch
+        for _ in range(warmup):
+            self.step(solver)
+        torch.cuda.synchronize()
+        times, launches = [], 0
+        stream = torch.cuda.ExternalStream(self.stream)
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, _, k = self.step(solver)
+            e1.record(stream)
+            launches += k
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        return float(np.mean(times)), launches
+
+    def host(self, kind):
+        t = self.d_first if kind == "first" else self.d_out
+        L = len(self.wl.layers)
+        return t.cpu().numpy().reshape(L, self.wl.height, self.wl.width, 4)
+
+
+def train_warm_start(U, torch, wl):
+    """The warm-start network for this layer set: 64 seeded 256x256 images
+    (2^22 pixels), batch 8192, 512 Adam steps at lr 1e-3."""
+    from unblending_b200 import synthetic as syn
+    modes = [s.mode for s in wl.layers]
+    t0 = time.perf_counter()
+    imgs = [syn.generate(256, 256, modes, (20.0, 200.0), seed=10_000 + k, layers=wl.layers) for k in range(64)]
+    d = [torch.from_numpy(w.image.reshape(-1)).cuda() for w in imgs]
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    model = U.mlp_train_device([(x.data_ptr(), 256, 256) for x in d], wl.layers, batch=8192, steps=512,
+                               learning_rate=1e-3, seed=1)
+    torch.cuda.synchronize()
+    return model, {"images": 64, "pixels": 64 * 256 * 256, "batch": 8192, "steps": 512, "lr": 1e-3,
+                   "final_batch_mse": model.loss, "train_s": time.perf_counter() - t0, "generate_s": t_gen}
+
+
 def b200_arm(args):
     import torch
-    rank, world, local = dist_env()
+    from unblending_b200 import dist
+    rank, world, local = dist.env()
     if world > 1:
-        import torch.distributed as dist
+        import datetime
+        import torch.distributed as tdist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     else:
         torch.cuda.set_device(0)
     import unblending_b200 as U
@@ -241,66 +310,55 @@ def b200_arm(args):
 
     wl = syn.workload(WORKLOAD, args.width, args.width, seed=2 + rank)
     L, n, w, h = len(wl.layers), wl.pixels, wl.width, wl.height
-    precision = U.PRECISION_FP64 if args.precision == "fp64" else U.PRECISION_FP32
-    so = U.solver_options(precision=precision)
     stream = torch.cuda.Stream()
-    d_img = torch.from_numpy(wl.image.reshape(-1)).cuda()
-    d_first = torch.empty(4 * L * n, dtype=torch.float64, device="cuda")
-    d_out = torch.empty_like(d_first)
-    d_status = torch.empty(n, dtype=torch.int32, device="cuda")
-    d_counters1 = torch.zeros((n, 5), dtype=torch.int32, device="cuda")
-    d_counters2 = torch.zeros((n, 5), dtype=torch.int32, device="cuda")
+    D = Decomposition(U, torch, wl, stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    sp = stream.cuda_stream
-
-    def step(counters=False, st=False):
-        s1 = U.unmix_device(w, h, d_img.data_ptr(), wl.layers, d_first.data_ptr(), solver=so,
-                            d_status=d_status.data_ptr(),
-                            d_counters=d_counters1.data_ptr() if counters else None, stream=sp, stats=st)
-        launches = U.last_launch_count()
-        s2 = U.refine_device(w, h, d_img.data_ptr(), wl.layers, d_first.data_ptr(), d_out.data_ptr(), smooth=True,
-                             solver=so, d_status=d_status.data_ptr(),
-                             d_counters=d_counters2.data_ptr() if counters else None, stream=sp, stats=st)
-        return s1, s2, launches + U.last_launch_count()
-
-    # Warm-up (also records stage timings and counters once).
-    s1 = s2 = None
-    for i in range(args.warmup):
-        s1, s2, _ = step(counters=(i == 0), st=True)
-    torch.cuda.synchronize()
+    plain = U.solver_options(precision=U.PRECISION_FP32)
 
     sampler = ClockSampler(local)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     sampler.start()
-    times, launches = [], 0
     wall0 = time.perf_counter()
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        _, _, k = step()
-        e1.record(stream)
-        launches += k
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-    torch.cuda.synchronize()
+    ms, launches = D.timed(plain, args.steps, args.warmup, flush)
     wall = time.perf_counter() - wall0
     clocks = sampler.stop()
-    ms = float(np.mean(times))
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world / (ms / 1e3)
+    value = dist.throughput(n, ms, "cuda")
+    ms_max = dist.reduce_max(ms, "cuda")
 
-    # Per-kernel breakdown of one step (device events inside the library).
-    s1, s2, _ = step(counters=True, st=True)
+    # Stage breakdown and work counters of one step.
+    s1, s2, _ = D.step(plain, counters=True, stats=True)
     torch.cuda.synchronize()
-    c1 = d_counters1.cpu().numpy().astype(np.int64)
-    c2 = d_counters2.cpu().numpy().astype(np.int64)
+    c1 = D.c1.cpu().numpy().astype(np.int64)
+    c2 = D.c2.cpu().numpy().astype(np.int64)
+    first_plain, final_plain = D.host("first"), D.host("final")
+
+    # ---- learned warm start on the first pass
+    warm = None
+    if not args.no_warm:
+        model, training = train_warm_start(U, torch, wl)
+        wsolver = U.solver_options(precision=U.PRECISION_FP32, warm_start=model)
+        wms, _ = D.timed(wsolver, args.steps, args.warmup, flush)
+        ws1, ws2, _ = D.step(wsolver, counters=True, stats=True)
+        torch.cuda.synchronize()
+        wc1 = D.c1.cpu().numpy().astype(np.int64)
+        warm = {"value": dist.throughput(n, wms, "cuda"), "ms_per_step": dist.reduce_max(wms, "cuda"),
+                "speedup_vs_plain": ms / wms, "training": training,
+                "unmix_counters_mean": wc1.mean(0).tolist(),
+                "stages_ms": {"unmix_solve": ws1["ms_solve"], "unmix_resolve_fp64": ws1["ms_resolve"],
+                              "filter": ws2["ms_filter"], "refine_solve": ws2["ms_solve"],
+                              "refine_resolve_fp64": ws2["ms_resolve"]},
+                "misses": {"unmix": ws1["misses"], "unmix_failed": ws1["failed"]}}
+        first_warm, final_warm = D.host("first"), D.host("final")
+
+    # ---- FP64 solve (replays the reference's FP64 solver)
+    fp64 = None
+    if not args.no_fp64:
+        fsolver = U.solver_options(precision=U.PRECISION_FP64)
+        fms, _ = D.timed(fsolver, max(2, args.steps // 2), 1, flush)
+        fp64 = {"value": dist.throughput(n, fms, "cuda"), "ms_per_step": dist.reduce_max(fms, "cuda")}
+        first_fp64, final_fp64 = D.host("first"), D.host("final")
 
     # ---- e2e through the C ABI with pinned host buffers
     host_img = torch.from_numpy(wl.image.copy()).pin_memory().numpy()
@@ -308,8 +366,7 @@ def b200_arm(args):
     host_out = torch.empty((L, h, w, 4), dtype=torch.float64).pin_memory().numpy()
     arr = syn.layer_array(wl.layers)
     view = U.RgbView(host_img.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), host_img.size, w, h, 0)
-    opts_unmix = U.options(True, False)
-    opts_refine = U.options(True, True)
+    opts_unmix, opts_refine = U.options(True, False), U.options(True, True)
     dp = ctypes.POINTER(ctypes.c_double)
 
     def e2e_step():
@@ -329,10 +386,6 @@ def b200_arm(args):
         e2e_step()
         e2e_times.append(time.perf_counter() - t0)
     e2e_ms = float(np.mean(e2e_times)) * 1e3
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
     h2d = 2 * host_img.nbytes + host_first.nbytes
     d2h = host_first.nbytes + host_out.nbytes
 
@@ -345,17 +398,16 @@ def b200_arm(args):
     achieved = (flops1 + flops2) / (solve_ms / 1e3) / 1e12
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
-    filter_bytes = 4 * (3 + 2 * (L + 3)) * n     # algorithmic bytes of the filter (f32 equivalent, by definition)
+    filter_bytes = 4 * (3 + 2 * (L + 3)) * n
     filter_gbs = filter_bytes / (s2["ms_filter"] / 1e3) / 1e9
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if precision == U.PRECISION_FP32 else "f64",
-        "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
         "config": {"workload": f"{WORKLOAD} {w}x{h} L=5 unmix+refine(opaque, smooth bg, r={s2['radius']})",
-                   "precision": args.precision, "warm_start": False, "starts": 1,
+                   "precision": "fp32 solve + fp64 check/re-solve of misses", "warm_start": False, "starts": 1,
                    "l2": "256 MiB buffer written between steps, outside the timed region",
                    "parallelism": f"{world} independent images (one per GPU)"},
         "clocks": clocks,
@@ -370,20 +422,25 @@ def b200_arm(args):
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": PEAK_FP32_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / PEAK_FP32_TFLOPS, "traffic": None,
                      "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json has no FP32 figure",
-                     "flops_per_step": flops1 + flops2},
+                     "flops_per_step": flops1 + flops2, "kernel": "solve_pixels<float,5,...>"},
         "roofline_filter": {"bound": "hbm", "achieved": filter_gbs, "peak": hbm_peak, "unit": "GB/s",
                             "frac": filter_gbs / hbm_peak, "algorithmic_bytes": filter_bytes,
                             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
-        "e2e": {"value": n * world / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        "warm_start": warm,
+        "fp64": fp64,
+        "e2e": {"value": dist.throughput(n, e2e_ms, "cuda"), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
     }
     if rank == 0 and not args.no_cpu_baseline:
         rng = np.random.default_rng(0)
         sample = np.sort(rng.choice(n, size=SAMPLE, replace=False))
-        first = d_first.cpu().numpy().reshape(L, h, w, 4)
-        final = d_out.cpu().numpy().reshape(L, h, w, 4)
+        finals = {"plain": (first_plain, final_plain)}
+        if warm is not None:
+            finals["warm_start"] = (first_warm, final_warm)
+        if fp64 is not None:
+            finals["fp64"] = (first_fp64, final_fp64)
         threads = os.cpu_count() or 1
-        sec, kind, details, parity = cpu_reference(wl, first, final, threads, sample)
+        sec, kind, details, parity = cpu_reference(wl, first_plain, finals, threads, sample)
         line["cpu_baseline"] = {"value": n / sec, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"CPU guided filter over the full image + both solves on {SAMPLE} seeded "
                                           f"pixels, extrapolated to {n} pixels", **details}

@@ -159,6 +159,32 @@ UNBLENDING_API int32_t unblending_unmix_device_noalloc(
     const unblending_options* options, const unblending_solver_options* solver,
     double* output, int32_t* status, void* stream);
 
+/* One image of a batched first pass. Device pointers: image (packed RGB
+ * doubles), output (packed [layer][row][column][RGBA] doubles), status (or
+ * NULL). Host pointers: layers (layer_count entries), warm_start (or NULL). */
+typedef struct unblending_image_job {
+    int32_t width, height;
+    const double* image;
+    const unblending_layer* layers;
+    int32_t layer_count;
+    double* output;
+    int32_t* status;
+    const unblending_mlp* warm_start;
+} unblending_image_job;
+
+/* First pass of many images of uneven size and layer count. No counterpart
+ * in the reference (which solves one image per call). Images are grouped by
+ * layer count; each group runs as one persistent launch whose work queue
+ * spans all its images' pixels, and all groups (with their warm-start
+ * inference and FP64 re-solves) are captured into one CUDA graph, replayed
+ * while the same job list is submitted again. The kernel variant and block
+ * size of each group come from a timing sweep on a pixel sample, cached per
+ * layer count. Results equal those of unblending_unmix_device per image.
+ * Synchronous when stats is non-NULL. */
+UNBLENDING_API int32_t unblending_unmix_batch_device(
+    const unblending_image_job* jobs, int32_t count, const unblending_options* options,
+    const unblending_solver_options* solver, void* stream, unblending_stats* stats);
+
 /* Number of GPU kernel launches the most recent call on this thread issued. */
 UNBLENDING_API int64_t unblending_last_launch_count(void);
 

@@ -33,7 +33,7 @@ EXPORTED = [
     "unblending_abi_version", "unblending_unmix", "unblending_refine", "unblending_unmix_ex",
     "unblending_refine_ex", "unblending_unmix_device", "unblending_refine_device", "unblending_last_launch_count",
     "unblending_unmix_device_noalloc", "unblending_mlp_train_device", "unblending_mlp_loss_grad_device",
-    "unblending_mlp_predict_device",
+    "unblending_mlp_predict_device", "unblending_unmix_batch_device",
 ]
 
 
@@ -81,6 +81,13 @@ class Mlp(ctypes.Structure):
 
     def set(self, name, value):
         np.ctypeslib.as_array(getattr(self, name))[:] = np.asarray(value, dtype=np.float32).reshape(-1)
+
+
+class ImageJob(ctypes.Structure):
+    """ctypes mirror of `unblending_image_job` (batched first pass)."""
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("image", ctypes.c_void_p),
+                ("layers", ctypes.c_void_p), ("layer_count", ctypes.c_int32), ("output", ctypes.c_void_p),
+                ("status", ctypes.c_void_p), ("warm_start", ctypes.c_void_p)]
 
 
 class MlpOptions(ctypes.Structure):
@@ -149,6 +156,9 @@ def _load():
     lib.unblending_mlp_predict_device.restype = ctypes.c_int32
     lib.unblending_mlp_predict_device.argtypes = [P(Mlp), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                                   ctypes.c_void_p, ctypes.c_void_p]
+    lib.unblending_unmix_batch_device.restype = ctypes.c_int32
+    lib.unblending_unmix_batch_device.argtypes = [ctypes.c_void_p, ctypes.c_int32, P(Options), P(SolverOptions),
+                                                  ctypes.c_void_p, P(Stats)]
     lib.unblending_unmix_device_noalloc.restype = ctypes.c_int32
     lib.unblending_unmix_device_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
@@ -316,6 +326,27 @@ def mlp_loss_grad_device(model: Mlp, count, d_features, d_targets) -> Mlp:
 
 def mlp_predict_device(model: Mlp, width, height, d_image, d_out, stream=None):
     _check(lib.unblending_mlp_predict_device(ctypes.byref(model), width, height, d_image, d_out, stream))
+
+
+def unmix_batch_device(jobs, opaque=True, solver=None, stream=None, stats=False):
+    """Batched first pass. jobs: list of dicts with width, height, d_image,
+    layers, d_output, and optional d_status, warm_start (Mlp)."""
+    arr = (ImageJob * len(jobs))()
+    keep = []
+    for k, j in enumerate(jobs):
+        layers, L = _layers(j["layers"])
+        keep.append(layers)
+        warm = j.get("warm_start")
+        if warm is not None:
+            keep.append(warm)
+        arr[k] = ImageJob(j["width"], j["height"], j["d_image"], ctypes.addressof(layers), L, j["d_output"],
+                          j.get("d_status"), ctypes.addressof(warm) if warm is not None else None)
+    st = Stats(); st.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_unmix_batch_device(arr, len(jobs), ctypes.byref(options(opaque)),
+                                           ctypes.byref(solver or solver_options()), stream,
+                                           ctypes.byref(st) if stats else None)
+    _check(rc)
+    return st.as_dict() if stats else None
 
 
 def last_launch_count() -> int:

@@ -28,7 +28,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.pat
 # (source, extra nvcc flags). The FP64 solver and the filter keep IEEE
 # multiply/add rounding (no FMA contraction) like the reference's CUDA build.
 UNITS = [
-    ("solver_fp32.cu", []),
+    ("solver_fp32.cu", ["--fmad=false"]),
     ("solver_fp64.cu", ["--fmad=false"]),
     ("filter.cu", ["--fmad=false"]),
     ("noalloc.cu", []),

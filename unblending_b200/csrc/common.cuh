@@ -60,6 +60,17 @@ struct SolverControls {
     int gradient_on_first_trial = 1;   // fuse the first line-search trial's gradient
 };
 
+// One image of a batched first pass: its pixels occupy global queue indices
+// [offset, offset + n) of its layer-count group.
+struct BatchJob {
+    const double* image;
+    double* out;
+    int32_t* status;
+    const float* warm;
+    int64_t offset, n;
+    int32_t model;      // index into the group's model table
+};
+
 // Everything one solve launch reads and writes. Device pointers only.
 //   image    : f64 interleaved RGB, pixel i at image[3*i .. 3*i+2]
 //   first    : refinement only, first pass packed f64 [l][i][RGBA]
@@ -83,6 +94,12 @@ struct SolveArgs {
     const int32_t* input_status = nullptr;  // refinement: nonzero = targets not normalizable (status 8, not solved)
     int32_t* input_failed = nullptr;        // count of such pixels
     const float* warm = nullptr;            // optional start-0 seed: n x 4L floats, pixel-major x
+    // Batched first pass: n is the group's total pixel count, pixels are
+    // global queue indices decoded through `jobs` (sorted by offset), and
+    // each job's layer models come from `models` (Models<T> entries).
+    const BatchJob* jobs = nullptr;
+    int job_count = 0;
+    const void* models = nullptr;
     int opaque = 1, smooth = 0;
 };
 

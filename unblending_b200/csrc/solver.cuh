@@ -127,7 +127,9 @@ template <class T, int L> struct History<T, L, true> {
 
 enum : int { kIdle = 0, kOuterEval = 1, kTrial = 2, kAcceptGrad = 3 };
 
-template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
+// BATCH: pixels of many images (one layer-count group); the quad's layer
+// models are staged in the shared-memory slot that `m` refers to.
+template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct QuadSolver {
     static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
     const Models<T>& m;
     const SolverControls& ctl;
@@ -137,7 +139,12 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
     T tol2, itol;
 
     // Per-pixel inputs (this lane's slice).
-    size_t pixel;
+    size_t pixel, gidx, npix;      // local pixel index, queue index, pixels of its image
+    const double* img;
+    double* outp;
+    int32_t* stp;
+    const float* wp;
+    int job_id = -1;
     double target64, bg64;
     T target, bgq;
     T ahat[R];           // alpha lane, refinement: filtered alpha targets (pinned alphas)
@@ -555,9 +562,9 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
     // ------------------------------------------------------------ pixels --
     // Loads pixel `i` and prepares start 0.
     __device__ __forceinline__ void load(size_t i) {
-        const size_t n = size_t(a.n);
+        const size_t n = npix;
         pixel = i;
-        target64 = colour ? a.image[3 * i + Q.q] : 0.0;
+        target64 = colour ? img[3 * i + Q.q] : 0.0;
         target = T(target64);
         bg64 = (REFINE && smooth && colour) ? a.targets[(size_t(L) + Q.q) * n + i] : 0.0;
         bgq = T(bg64);
@@ -575,10 +582,10 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
             } else {
                 init[l] = (opaque && l == 0) ? T(1) : (REFINE ? ahat[REFINE ? l : 0] : T(0.5));
             }
-            if (!REFINE && a.warm) {
+            if (!REFINE && wp) {
                 // Learned warm start: the network's prediction replaces the
                 // start-0 seed (bounds still apply when the start is seeded).
-                const float* wv = a.warm + i * size_t(4 * L);
+                const float* wv = wp + i * size_t(4 * L);
                 init[l] = T(colour ? wv[L + 3 * l + Q.q] : wv[l]);
             }
         }
@@ -591,7 +598,7 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
     // Writes the finished pixel: output (pinned values exactly), FP64
     // feasibility check, status, miss list, counters.
     __device__ __forceinline__ void store(bool skipped) {
-        const size_t n = size_t(a.n), i = pixel;
+        const size_t n = npix, i = pixel;
         double v[L], ah[R];
 #pragma unroll
         for (int l = 0; l < R; ++l) {
@@ -605,7 +612,7 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
             if (REFINE && !colour) v[l] = ah[REFINE ? l : 0];
             if (REFINE && smooth && colour && l == 0) v[l] = bg64;
             if (!REFINE && opaque && !colour && l == 0) v[l] = 1.0;
-            a.out[(size_t(l) * n + i) * 4 + Q.q] = v[l];
+            outp[(size_t(l) * n + i) * 4 + Q.q] = v[l];
         }
         // FP64 constraint check of the written point (solver_workspace.cuh:18-38).
         double av[L];
@@ -633,14 +640,14 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
         const bool miss = !(norm < ctl.outer_tolerance * ctl.outer_tolerance);
         if (Q.q == 0) {
             if (skipped) {
-                if (a.status) a.status[i] = 8;
+                if (stp) stp[i] = 8;
                 if (a.input_failed) atomicAdd(a.input_failed, 1);
             } else {
-                if (a.status) a.status[i] = miss ? 3 : 0;
-                if (miss && a.miss_list) a.miss_list[atomicAdd(a.miss_count, 1)] = int32_t(i);
+                if (stp) stp[i] = miss ? 3 : 0;
+                if (miss && a.miss_list) a.miss_list[atomicAdd(a.miss_count, 1)] = int32_t(gidx);
             }
             if (a.counters) {
-                uint32_t* cnt = a.counters + 5 * i;
+                uint32_t* cnt = a.counters + 5 * gidx;
                 cnt[0] = n_values; cnt[1] = n_gradients; cnt[2] = n_iterations; cnt[3] = n_backtracks; cnt[4] = n_outer;
             }
         }
@@ -654,7 +661,29 @@ template <class T, int L, bool REFINE, bool HSMEM> struct QuadSolver {
             if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
             job = Q.from(job, 0);
             if (job >= total) { phase = kIdle; return false; }
-            const size_t i = size_t(a.list ? a.list[job] : job);
+            gidx = size_t(a.list ? a.list[job] : job);
+            size_t i = gidx;
+            if (BATCH) {
+                // The image owning queue index gidx: last job with offset <= gidx.
+                int lo = 0, hi = a.job_count - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (a.jobs[mid].offset <= int64_t(gidx)) lo = mid; else hi = mid - 1;
+                }
+                const BatchJob& J = a.jobs[lo];
+                if (lo != job_id) {
+                    // Stage this image's layer models in the quad's slot (a
+                    // typed copy: the solver reads the fields with their types).
+                    __syncwarp(Q.mask);
+                    if (Q.q == 0) const_cast<Models<T>&>(m) = static_cast<const Models<T>*>(a.models)[J.model];
+                    __syncwarp(Q.mask);
+                    job_id = lo;
+                }
+                img = J.image; outp = J.out; stp = J.status; wp = J.warm; npix = size_t(J.n);
+                i = gidx - size_t(J.offset);
+            } else {
+                img = a.image; outp = a.out; stp = a.status; wp = a.warm; npix = size_t(a.n);
+            }
             load(i);
             if (REFINE && a.input_status && a.input_status[i] != 0) {
                 // Targets that cannot be normalized: keep the initial layers

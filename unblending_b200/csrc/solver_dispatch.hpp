@@ -13,6 +13,12 @@ cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<floa
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
 cudaError_t launch_solve_fp64(int L, bool refine, const Models<double>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
+// Batched first pass over the images of one layer-count group
+// (SolveArgs::jobs / models); variant 0 or 2 as above.
+cudaError_t launch_solve_batch_fp32(int L, int variant, const SolverControls& c, const SolveArgs& a, int threads,
+                                    int sms, cudaStream_t s);
+cudaError_t launch_solve_batch_fp64(int L, const SolverControls& c, const SolveArgs& a, int threads, int sms,
+                                    cudaStream_t s);
 
 // Guided-filter refinement targets, FP64 throughout.
 struct FilterArgs {

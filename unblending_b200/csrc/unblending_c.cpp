@@ -60,9 +60,30 @@ struct Buffer {
     }
 };
 
+// A batched first pass captured as a CUDA graph, with the device tables and
+// scratch it refers to; replayed while the same job list comes back.
+struct BatchPlan {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::unique_ptr<Buffer>> buffers;
+    std::vector<int32_t*> counts;   // per group: [0] misses, [1] failures
+    int64_t pixels = 0;
+    int launches = 0;
+    BatchPlan() = default;
+    BatchPlan(const BatchPlan&) = delete;
+    BatchPlan& operator=(const BatchPlan&) = delete;
+    ~BatchPlan() { if (exec) cudaGraphExecDestroy(exec); }
+    template <class T> T* alloc(size_t count) {
+        buffers.push_back(std::make_unique<Buffer>());
+        return buffers.back()->get<T>(count);
+    }
+};
+
 // One per CUDA device: a stream, the solver's scratch, and timing events.
 // Calls on the same device are serialized by `mutex`.
 struct Context {
+    std::unique_ptr<BatchPlan> plan;
+    std::map<std::pair<int, int>, std::pair<int, int>> tuned;   // (L, precision) -> (variant, threads)
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
@@ -556,6 +577,244 @@ int32_t unblending_refine_device(int32_t width, int32_t height, const double* im
 }
 
 int64_t unblending_last_launch_count(void) { return t_launches; }
+
+int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t count, const unblending_options* options,
+                                      const unblending_solver_options* solver, void* stream, unblending_stats* stats) {
+    t_launches = 0;
+    if (!jobs || count < 1) return UNBLENDING_INVALID_ARGUMENT;
+    if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
+    unblending_solver_options so;
+    int32_t rc = resolve_solver(solver, so);
+    if (rc != UNBLENDING_OK) return rc;
+    std::vector<Spec> specs(count);
+    std::map<int, std::vector<int>> groups;   // layer count -> jobs
+    std::map<int, const unblending_mlp*> group_model;
+    for (int k = 0; k < count; ++k) {
+        const auto& J = jobs[k];
+        unblending_rgb_view view{J.image, 0, J.width, J.height, 0};
+        if (J.layer_count < 1) return UNBLENDING_INVALID_ARGUMENT;
+        rc = validate(&view, J.layers, size_t(J.layer_count), options, J.output, 0, false, nullptr, 0, specs[k], true);
+        if (rc != UNBLENDING_OK) return rc;
+        if (J.warm_start) {
+            if (!mlp_valid(J.warm_start, J.layer_count)) return UNBLENDING_INVALID_ARGUMENT;
+            auto it = group_model.find(J.layer_count);
+            // One network per layer count within a batch.
+            if (it != group_model.end() && it->second != J.warm_start) return UNBLENDING_INVALID_ARGUMENT;
+            group_model[J.layer_count] = J.warm_start;
+        }
+        groups[J.layer_count].push_back(k);
+    }
+    // Plan key: everything the captured graph depends on.
+    std::vector<unsigned char> key;
+    auto put = [&](const void* p, size_t bytes) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        key.insert(key.end(), b, b + bytes);
+    };
+    put(&count, sizeof(count));
+    put(&stream, sizeof(stream));
+    put(&so, offsetof(unblending_solver_options, warm_start));
+    for (int k = 0; k < count; ++k) {
+        const auto& J = jobs[k];
+        put(&J.width, sizeof(J.width)); put(&J.height, sizeof(J.height));
+        put(&J.image, sizeof(J.image)); put(&J.output, sizeof(J.output)); put(&J.status, sizeof(J.status));
+        put(&J.layer_count, sizeof(J.layer_count));
+        put(J.layers, sizeof(unblending_layer) * size_t(J.layer_count));
+        const bool warm = J.warm_start != nullptr;
+        put(&warm, sizeof(warm));
+        if (warm) put(J.warm_start, sizeof(unblending_mlp));
+    }
+    return guarded([&]() -> int32_t {
+        Context& c = context();
+        std::lock_guard<std::mutex> lock(c.mutex);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+        if (!c.plan || c.plan->key != key) {
+            c.plan.reset();
+            auto plan = std::make_unique<BatchPlan>();
+            plan->key = key;
+            SolverControls ctl;
+            ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
+            ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+            struct Group {
+                int L;
+                SolveArgs fp, re;      // first solve (warm where given), FP64 re-solve (reference start)
+                uint32_t* queues;
+                int32_t* counts;
+                std::vector<std::pair<int, float*>> infer;   // job, warm slice
+                MlpDevice net;
+                int variant = 0, threads = 128;
+            };
+            std::vector<Group> gs;
+            for (auto& [L, members] : groups) {
+                Group G;
+                G.L = L;
+                std::vector<BatchJob> table, cold;
+                std::vector<Models<float>> m32;
+                std::vector<Models<double>> m64;
+                int64_t off = 0;
+                const unblending_mlp* net = group_model.count(L) ? group_model[L] : nullptr;
+                float* warm = nullptr;
+                int64_t total = 0;
+                for (int k : members) total += int64_t(specs[k].pixels);
+                if (net) warm = plan->alloc<float>(size_t(total) * 4 * L);
+                for (int k : members) {
+                    const auto& J = jobs[k];
+                    BatchJob b;
+                    b.image = J.image; b.out = J.output; b.status = J.status;
+                    b.offset = off; b.n = int64_t(specs[k].pixels); b.model = int32_t(table.size());
+                    b.warm = nullptr;
+                    cold.push_back(b);
+                    if (J.warm_start) {
+                        b.warm = warm + off * 4 * L;
+                        G.infer.emplace_back(k, const_cast<float*>(b.warm));
+                    }
+                    table.push_back(b);
+                    m32.push_back(make_models<float>(J.layers, L));
+                    m64.push_back(make_models<double>(J.layers, L));
+                    off += b.n;
+                }
+                if (net) {
+                    // The group's own device copy of its network (the graph keeps referring to it).
+                    const MlpDevice shared = upload_model(c, *net, s);
+                    __nv_bfloat16* w = plan->alloc<__nv_bfloat16>(mlp_weight_count());
+                    float* bb = plan->alloc<float>(mlp_bias_count());
+                    ck(cudaMemcpyAsync(w, shared.w[0], mlp_weight_count() * sizeof(__nv_bfloat16),
+                                       cudaMemcpyDeviceToDevice, s));
+                    ck(cudaMemcpyAsync(bb, shared.b[0], mlp_bias_count() * sizeof(float), cudaMemcpyDeviceToDevice, s));
+                    for (int q = 0; q < 4; ++q) {
+                        G.net.w[q] = w + (shared.w[q] - shared.w[0]);
+                        G.net.b[q] = bb + (shared.b[q] - shared.b[0]);
+                    }
+                }
+                BatchJob* d_table = plan->alloc<BatchJob>(2 * table.size());
+                Models<float>* d_m32 = plan->alloc<Models<float>>(m32.size());
+                Models<double>* d_m64 = plan->alloc<Models<double>>(m64.size());
+                ck(cudaMemcpyAsync(d_table, table.data(), table.size() * sizeof(BatchJob), cudaMemcpyHostToDevice, s));
+                ck(cudaMemcpyAsync(d_table + table.size(), cold.data(), cold.size() * sizeof(BatchJob),
+                                   cudaMemcpyHostToDevice, s));
+                ck(cudaMemcpyAsync(d_m32, m32.data(), m32.size() * sizeof(Models<float>), cudaMemcpyHostToDevice, s));
+                ck(cudaMemcpyAsync(d_m64, m64.data(), m64.size() * sizeof(Models<double>), cudaMemcpyHostToDevice, s));
+                ck(cudaStreamSynchronize(s));   // host tables go out of scope
+                G.queues = plan->alloc<uint32_t>(8);
+                G.counts = reinterpret_cast<int32_t*>(G.queues + 4);
+                int32_t* lists = plan->alloc<int32_t>(2 * size_t(total));
+                SolveArgs& a = G.fp;
+                a.n = int(total);
+                a.jobs = d_table; a.job_count = int(table.size());
+                a.opaque = specs[members[0]].opaque; a.smooth = 0;
+                a.queue = G.queues;
+                a.miss_list = lists; a.miss_count = G.counts + 0;
+                SolveArgs& b = G.re;
+                b = a;
+                b.jobs = d_table + table.size();
+                b.models = d_m64;
+                b.list = lists; b.list_count = G.counts + 0;
+                b.miss_list = lists + total; b.miss_count = G.counts + 1;
+                b.queue = G.queues + 1;
+                a.models = so.precision == UNBLENDING_PRECISION_FP64 ? static_cast<const void*>(d_m64) : d_m32;
+                if (so.precision == UNBLENDING_PRECISION_FP64) a.miss_count = G.counts + 1;
+                plan->counts.push_back(G.counts);
+                plan->pixels += total;
+                // Autotuner: time each FP32 kernel variant / block size on a
+                // sample of this group's pixels spread over its images.
+                const auto tkey = std::make_pair(L, so.precision);
+                if (so.precision == UNBLENDING_PRECISION_FP32 && so.threads_per_block == 0 && so.kernel_variant < 0) {
+                    if (!c.tuned.count(tkey)) {
+                        const int S = int(std::min<int64_t>(total, 8192));
+                        std::vector<int32_t> sample(S);
+                        for (int q = 0; q < S; ++q) sample[q] = int32_t(int64_t(q) * total / S);
+                        int32_t* d_sample = plan->alloc<int32_t>(S);
+                        int32_t* d_count = plan->alloc<int32_t>(1);
+                        ck(cudaMemcpyAsync(d_sample, sample.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+                        ck(cudaMemcpyAsync(d_count, &S, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+                        const std::pair<int, int> candidates[3] = {{0, 128}, {2, 128}, {0, 64}};
+                        float best_ms = 1e30f;
+                        std::pair<int, int> best = candidates[0];
+                        for (const auto& cand : candidates) {
+                            SolveArgs t = a;
+                            t.jobs = d_table + table.size();   // reference start: the network has not run yet
+                            t.list = d_sample; t.list_count = d_count;
+                            t.miss_list = nullptr; t.status = nullptr;
+                            ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
+                            ck(cudaEventRecord(c.ev[4], s));
+                            ck(launch_solve_batch_fp32(L, cand.first, ctl, t, cand.second, c.sms, s));
+                            ck(cudaEventRecord(c.ev[5], s));
+                            ck(cudaEventSynchronize(c.ev[5]));
+                            const float ms = elapsed(c.ev[4], c.ev[5]);
+                            if (ms < best_ms) { best_ms = ms; best = cand; }
+                        }
+                        c.tuned[tkey] = best;
+                    }
+                    G.variant = c.tuned[tkey].first;
+                    G.threads = c.tuned[tkey].second;
+                } else {
+                    G.variant = so.kernel_variant >= 0 ? so.kernel_variant : 0;
+                    G.threads = so.threads_per_block ? so.threads_per_block : 128;
+                    if (G.variant == 1) G.variant = 2;   // batch kernels: register or 3-block shared history
+                }
+                gs.push_back(G);
+            }
+            // Capture every group's work into one graph.
+            cudaGraph_t graph = nullptr;
+            ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+            int launches = 0;
+            try {
+                for (auto& G : gs) {
+                    ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
+                    for (auto& [k, w] : G.infer) {
+                        ck(launch_mlp_infer(G.net, jobs[k].image, jobs[k].width, jobs[k].height, G.L, w, G.counts + 3,
+                                            c.sms, s));
+                        ++launches;
+                    }
+                    if (so.precision == UNBLENDING_PRECISION_FP64) {
+                        ck(launch_solve_batch_fp64(G.L, ctl, G.fp, 128, c.sms, s));
+                        ++launches;
+                    } else {
+                        ck(launch_solve_batch_fp32(G.L, G.variant, ctl, G.fp, G.threads, c.sms, s));
+                        ++launches;
+                        if (so.resolve_misses) {
+                            ck(launch_solve_batch_fp64(G.L, ctl, G.re, 128, c.sms, s));
+                            ++launches;
+                        } else {
+                            ck(cudaMemcpyAsync(G.counts + 1, G.counts, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+                        }
+                    }
+                }
+            } catch (...) {
+                cudaStreamEndCapture(s, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            ck(cudaStreamEndCapture(s, &graph));
+            cudaError_t e = cudaGraphInstantiate(&plan->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            ck(e);
+            plan->launches = launches;
+            c.plan = std::move(plan);
+        }
+        BatchPlan& P = *c.plan;
+        ck(cudaEventRecord(c.ev[0], s));
+        ck(cudaGraphLaunch(P.exec, s));
+        ck(cudaEventRecord(c.ev[1], s));
+        t_launches = P.launches;
+        if (stats) {
+            int64_t misses = 0, failed = 0;
+            for (int32_t* cnt : P.counts) {
+                int32_t h[2];
+                ck(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+                ck(cudaStreamSynchronize(s));
+                misses += h[0]; failed += h[1];
+            }
+            *stats = unblending_stats{};
+            stats->struct_size = sizeof(unblending_stats);
+            stats->pixels = P.pixels;
+            stats->misses = misses; stats->failed = failed;
+            stats->ms_solve = elapsed(c.ev[0], c.ev[1]);
+            stats->ms_total = stats->ms_solve;
+        }
+        ck(cudaPeekAtLastError());
+        return UNBLENDING_OK;
+    });
+}
 
 int32_t unblending_mlp_predict_device(const unblending_mlp* model, int32_t width, int32_t height, const double* image,
                                       float* out, void* stream) {

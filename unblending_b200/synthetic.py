@@ -227,6 +227,30 @@ def workload(name: str, width: int | None = None, height: int | None = None, see
     return generate(name=name, **cfg)
 
 
+BATCH_MODES = [M["normal"], M["multiply"], M["screen"], M["overlay"], M["color_dodge"], M["soft_light"],
+               M["color_burn"]]
+
+
+def batch(count: int = 64, seed: int = 4, sides: tuple[int, int] = (256, 2048),
+          layers: tuple[int, int] = (3, 6)) -> list[Workload]:
+    """Images of uneven size and layer count: side ~ U{sides}, aspect 1:1 to
+    4:3 (either orientation), L ~ U{layers}, modes drawn from normal,
+    multiply, screen, overlay, color-dodge, soft-light, color-burn (bottom
+    layer normal), blobs 20-200 px, each image with its own seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        side = int(rng.integers(sides[0], sides[1] + 1))
+        aspect = rng.uniform(1.0, 4.0 / 3.0)
+        w, h = side, max(1, int(round(side / aspect)))
+        if rng.random() < 0.5:
+            w, h = h, w
+        L = int(rng.integers(layers[0], layers[1] + 1))
+        modes = [M["normal"]] + [int(m) for m in rng.choice(BATCH_MODES, size=L - 1)]
+        out.append(generate(w, h, modes, (20.0, 200.0), seed=int(rng.integers(1 << 31)), name=f"batch{k}"))
+    return out
+
+
 def reference_radius(width: int, height: int) -> int:
     """The reference's refinement radius, 60 * min(w, h) / 1000 (unblending.cpp:351)."""
     return 60 * min(width, height) // 1000
