@@ -38,13 +38,15 @@ typedef struct unblending_solver_options {
     double inner_tolerance;     /* default 5e-3 */
     double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
     int32_t threads_per_block;  /* 0 selects the tuned default */
-    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1/2 in shared memory
-                                   with registers capped for 4/3 blocks per SM */
+    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1..4 in shared memory
+                                   with registers capped for 4, 3, 5, 6 blocks per SM */
     const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start */
+    int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default, 0 uncapped registers, 1/2 capped for
+                                   2/3 blocks per SM */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

@@ -25,11 +25,12 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 
-# (source, extra nvcc flags). The FP64 solver and the filter keep IEEE
-# multiply/add rounding (no FMA contraction) like the reference's CUDA build.
+# (source, extra nvcc flags). The solver (one unit per layer count) and the
+# filter keep IEEE multiply/add rounding (no FMA contraction) like the
+# reference's CUDA build.
 UNITS = [
-    ("solver_fp32.cu", ["--fmad=false"]),
-    ("solver_fp64.cu", ["--fmad=false"]),
+    *[(f"solver_l{L}.cu", ["--fmad=false"]) for L in range(1, 9)],
+    ("solver_launch.cu", []),
     ("filter.cu", ["--fmad=false"]),
     ("noalloc.cu", []),
     ("mlp.cu", []),

@@ -16,27 +16,30 @@
 // (x = alpha_l). Every vector of the method (x, gradient, direction, trial
 // point, best point, the L-BFGS history) is split the same way, so dot
 // products are a local sum plus two xor-shuffles and each lane keeps only L
-// values of every vector: with L a template parameter all of it stays in
-// registers (the FP64 build keeps its history in shared memory instead). The
-// composite is separable per channel given the alphas, which lane 3
-// broadcasts; the 3x3 colour prior needs the three deltas of a layer (two
-// shuffles); the adjoint sweep reduces the alpha sensitivities of the three
-// channels once per layer. Every branch is taken on quad-uniform values, so a
-// quad never splits.
+// values of every vector. The five vectors the inner loop touches on every
+// step (x, gradient, direction, trial point, trial gradient) live in
+// registers; the cold ones (best point, the outer step's start point, the
+// start-0 seed) and the work counters live in a per-lane shared-memory slice,
+// and so does the L-BFGS history in the shared-history variants (the
+// register variant keeps it as a shift register). The composite is separable
+// per channel given the alphas, which lane 3 broadcasts; the 3x3 colour prior
+// needs the three deltas of a layer (two shuffles); the adjoint sweep reduces
+// the alpha sensitivities of the three channels once per layer. Every branch
+// is taken on quad-uniform values, so a quad never splits.
 //
-// Lockstep: the method is run as a state machine in which every step of the
-// warp's loop performs exactly one objective evaluation per quad (the
-// gradient half predicated on the quads that need it), followed by the
-// evaluation-free bookkeeping of that quad's phase (line-search decision,
-// L-BFGS update and two-loop recursion, multiplier update). The eight pixels
-// of a warp therefore share one instruction stream for the expensive part
-// instead of serializing through different phases, and the evaluator has a
-// single call site (one copy in the instruction cache). A quad whose pixel is
-// finished pulls the next pixel from an atomic queue inside the loop; the warp
-// leaves the loop when every quad is idle. The evaluated points and every
-// decision are those of the reference method, step for step; the one
-// evaluation left out is the re-evaluation at the end of an outer step, at a
-// point already evaluated, whose residual the state keeps instead.
+// Lockstep: every trip of the warp's loop performs exactly one objective
+// evaluation per quad (the gradient half predicated on the quads that need
+// it), followed by the evaluation-free bookkeeping of that quad. The
+// bookkeeping is a small action machine (begin iteration, next line-search
+// trial, accept, end of an outer step, begin start, begin outer step, store,
+// fetch) run until the quad needs its next evaluation; each action's code
+// exists once in the kernel, which keeps the loop's instruction footprint
+// small enough for the instruction cache. A quad whose pixel is finished
+// pulls the next pixel from an atomic queue; the warp leaves the loop when
+// every quad is idle. The evaluated points and every decision are those of
+// the reference method, step for step; the one evaluation left out is the
+// re-evaluation at the end of an outer step, at a point already evaluated,
+// whose residual the state keeps instead.
 #pragma once
 #include "blend.cuh"
 #include "common.cuh"
@@ -48,6 +51,17 @@ template <class T> __device__ __forceinline__ T sel3(int q, T a, T b, T c) { ret
 template <class T> __device__ __forceinline__ bool finite_(T v);
 template <> __device__ __forceinline__ bool finite_<float>(float v) { return isfinite(v); }
 template <> __device__ __forceinline__ bool finite_<double>(double v) { return isfinite(v); }
+
+// Blend value on cold paths (the third start's seeding), kept out of line so
+// that its switch over the modes is not copied into every unrolled layer.
+template <class T> __device__ __noinline__ T blend_value_cold(int mode, T s, T d) { return blend_value<T>(mode, s, d); }
+
+// Dynamic shared memory of the solve kernels (one declaration for all of
+// them; addressed by thread index, so no pointer stays live in registers).
+extern __shared__ __align__(16) unsigned char solver_smem[];
+// Lane stride of the per-lane slices: the largest block (128 threads), so
+// that slice offsets are compile-time constants for any block size.
+constexpr int kSliceStride = 128;
 
 struct Quad {
     unsigned mask;
@@ -88,12 +102,14 @@ struct Quad {
 };
 
 // L-BFGS pairs, indexed by age j (0 = newest). Register form: a shift
-// register with compile-time indices. Shared-memory form: a ring buffer.
+// register with compile-time indices. Shared-memory form: a ring buffer in
+// the lane's slice after its cold values, element (slot, l, s|y) at
+// slice index 3L + (slot*L + l)*2 + w.
 template <class T, int L, bool SMEM> struct History;
 
 template <class T, int L> struct History<T, L, false> {
     T s_[kHistory][L], y_[kHistory][L];
-    __device__ __forceinline__ void init(T*) {}
+    __device__ __forceinline__ void init() {}
     __device__ __forceinline__ T s(int j, int l) const { return s_[j][l]; }
     __device__ __forceinline__ T y(int j, int l) const { return y_[j][l]; }
     __device__ __forceinline__ void push(const T* sv, const T* yv) {
@@ -108,68 +124,128 @@ template <class T, int L> struct History<T, L, false> {
 };
 
 template <class T, int L> struct History<T, L, true> {
-    T* base;   // this lane's slice: element (slot, l, s|y) at base[((slot*L + l)*2 + w) * blockDim.x]
+    static constexpr int kBase = 3 * L;   // after the lane slice's cold values
     int next;
-    __device__ __forceinline__ void init(T* smem) { base = smem + threadIdx.x; next = 0; }
-    __device__ __forceinline__ int slot(int j) const { int k = next - 1 - j; return k < 0 ? k + kHistory : k; }
-    __device__ __forceinline__ T s(int j, int l) const { return base[size_t((slot(j) * L + l) * 2) * blockDim.x]; }
-    __device__ __forceinline__ T y(int j, int l) const { return base[size_t((slot(j) * L + l) * 2 + 1) * blockDim.x]; }
+    // This lane's pair of age j: element l of s at row(j)[2*l*kSliceStride],
+    // of y at row(j)[(2*l + 1)*kSliceStride].
+    __device__ __forceinline__ T* row(int j) const {
+        int k = next - 1 - j;
+        k = k < 0 ? k + kHistory : k;
+        return reinterpret_cast<T*>(solver_smem) + (kBase + k * 2 * L) * kSliceStride + threadIdx.x;
+    }
+    __device__ __forceinline__ void init() { next = 0; }
+    __device__ __forceinline__ T s(int j, int l) const { return row(j)[2 * l * kSliceStride]; }
+    __device__ __forceinline__ T y(int j, int l) const { return row(j)[(2 * l + 1) * kSliceStride]; }
     __device__ __forceinline__ void push(const T* sv, const T* yv) {
+        T* p = reinterpret_cast<T*>(solver_smem) + (kBase + next * 2 * L) * kSliceStride + threadIdx.x;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            base[size_t((next * L + l) * 2) * blockDim.x] = sv[l];
-            base[size_t((next * L + l) * 2 + 1) * blockDim.x] = yv[l];
+            p[2 * l * kSliceStride] = sv[l];
+            p[(2 * l + 1) * kSliceStride] = yv[l];
         }
         next = next + 1 == kHistory ? 0 : next + 1;
     }
     __device__ __forceinline__ void reset() { next = 0; }
 };
 
+// Per-lane shared-memory slice of the solver: kValues values of T (cold
+// values; with HSMEM the L-BFGS history and the two-loop coefficients), then
+// kCounters uint32 work counters; element k of a lane at
+// [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
+// A batched launch places one layer-model slot per quad after the slices.
+template <class T, int L, bool HSMEM> struct LaneSlice {
+    static constexpr int kCold = 3 * L;                                  // best, outer-start point, start-0 seed
+    static constexpr int kCoeff = kCold + 2 * kHistory * L;              // two-loop coefficients (HSMEM)
+    static constexpr int kValues = HSMEM ? kCoeff + 2 * kHistory : kCold;
+    static constexpr int kCounters = 5;
+    __device__ __forceinline__ static T& value(int k) {
+        return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
+    }
+    __device__ __forceinline__ static uint32_t& counter(int k) {
+        return reinterpret_cast<uint32_t*>(solver_smem + value_bytes())[k * kSliceStride + threadIdx.x];
+    }
+    __host__ __device__ static constexpr size_t value_bytes() {
+        return (size_t(kSliceStride) * kValues * sizeof(T) + 15) / 16 * 16;
+    }
+    __host__ __device__ static constexpr size_t bytes() {
+        return value_bytes() + (size_t(kSliceStride) * kCounters * sizeof(uint32_t) + 15) / 16 * 16;
+    }
+};
+
 enum : int { kIdle = 0, kOuterEval = 1, kTrial = 2, kAcceptGrad = 3 };
+// Bookkeeping actions; aEval hands the quad to the next evaluation.
+enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart, aBeginOuter, aFinish, aFetch };
 
 // BATCH: pixels of many images (one layer-count group); the quad's layer
 // models are staged in the shared-memory slot that `m` refers to.
 template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct QuadSolver {
     static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
-    const Models<T>& m;
+    using Slice = LaneSlice<T, L, HSMEM>;
+    const Models<T>* models_;
     const SolverControls& ctl;
     const SolveArgs& a;
     Quad Q;
     bool colour, opaque, smooth;
     T tol2, itol;
 
-    // Per-pixel inputs (this lane's slice).
-    size_t pixel, gidx, npix;      // local pixel index, queue index, pixels of its image
-    const double* img;
-    double* outp;
-    int32_t* stp;
-    const float* wp;
+    // Current pixel (this lane's slice of it).
+    int pixel = 0, gidx = 0;   // pixel index within its image, queue index
     int job_id = -1;
-    double target64, bg64;
     T target, bgq;
     T ahat[R];           // alpha lane, refinement: filtered alpha targets (pinned alphas)
-    T init[L];           // start-0 seed before clamping
 
     // Method state (this lane's slice).
-    T x[L], g[L], d[L], tr[L], ng[L], ox[L], best[L];
+    T x[L], g[L], d[L], tr[L], ng[L];
     T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
     History<T, L, HSMEM> hist;
 
     // Per-quad scalars (uniform within the quad).
     int phase, start, outer, it, attempt, bt, valid;
-    T rho, f, oldnorm, step, slope;
+    T rho, f, oldnorm, step, slope, cand;
     T best_norm, best_energy;
     bool have_best;
-    uint32_t n_values, n_gradients, n_iterations, n_backtracks, n_outer;
 
-    __device__ QuadSolver(const Models<T>& models, const SolverControls& c, const SolveArgs& args)
-        : m(models), ctl(c), a(args) {
+    __device__ QuadSolver(const Models<T>* models, const SolverControls& c, const SolveArgs& args)
+        : models_(models), ctl(c), a(args) {
         colour = Q.q < 3;
         opaque = a.opaque != 0;
         smooth = a.smooth != 0;
         tol2 = T(ctl.outer_tolerance * ctl.outer_tolerance);
         itol = T(ctl.inner_tolerance);
         phase = kIdle;
+        hist.init();
+    }
+
+    // The layer models: the kernel parameter, or the quad's shared-memory
+    // slot in a batched launch.
+    __device__ __forceinline__ const Models<T>& models() const {
+        if constexpr (BATCH)
+            return reinterpret_cast<const Models<T>*>(solver_smem + Slice::bytes())[threadIdx.x >> 2];
+        else return *models_;
+    }
+
+    // ------------------------------------------------------ cold values --
+    __device__ __forceinline__ T& best(int l) const { return Slice::value(l); }
+    __device__ __forceinline__ T& ox(int l) const { return Slice::value(L + l); }
+    __device__ __forceinline__ T& init(int l) const { return Slice::value(2 * L + l); }
+    __device__ __forceinline__ uint32_t& counter(int k) const { return Slice::counter(k); }
+    __device__ __forceinline__ void count(int k) const { if (a.counters) ++counter(k); }
+
+    // ------------------------------------------------- image accessors --
+    __device__ __forceinline__ const double* image() const {
+        if constexpr (BATCH) return a.jobs[job_id].image; else return a.image;
+    }
+    __device__ __forceinline__ double* output() const {
+        if constexpr (BATCH) return a.jobs[job_id].out; else return a.out;
+    }
+    __device__ __forceinline__ int32_t* status() const {
+        if constexpr (BATCH) return a.jobs[job_id].status; else return a.status;
+    }
+    __device__ __forceinline__ const float* warm() const {
+        if constexpr (BATCH) return a.jobs[job_id].warm; else return a.warm;
+    }
+    __device__ __forceinline__ size_t pixels() const {
+        if constexpr (BATCH) return size_t(a.jobs[job_id].n); else return size_t(a.n);
     }
 
     // ------------------------------------------------------------ bounds --
@@ -191,18 +267,18 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         const T lv = lo(l), hv = hi(l);
         return lv == hv || (x[l] <= lv && gl > T(0)) || (x[l] >= hv && gl < T(0));
     }
-    __device__ __forceinline__ T mean_of(int l) const {
+    __device__ __forceinline__ T mean_of(const Models<T>& m, int l) const {
         return colour ? sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
     }
 
     // FP32: table-driven blend and reciprocal-based division; FP64: the
     // reference's formulas with IEEE division.
     static constexpr bool kFast = sizeof(T) == 4;
-    __device__ __forceinline__ T blend(int l, T s, T d) const {
+    __device__ __forceinline__ T blend(const Models<T>& m, int l, T s, T d) const {
         if constexpr (kFast) { T f, fs, fd; blend_table<T>(m, l, s, d, f, fs, fd, false); return f; }
         else return blend_value<T>(m.mode[l], s, d);
     }
-    __device__ __forceinline__ void blend3(int l, T s, T d, T& f, T& fs, T& fd) const {
+    __device__ __forceinline__ void blend3(const Models<T>& m, int l, T s, T d, T& f, T& fs, T& fd) const {
         if constexpr (kFast) blend_table<T>(m, l, s, d, f, fs, fd, true);
         else blend_all<T>(m.mode[l], s, d, f, fs, fd);
     }
@@ -218,6 +294,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     // Evaluates the AL value at tr (uniform across the quad), sets res[] and,
     // when need_grad, the gradient slice ng[]. Tracks the best feasible point.
     __device__ __forceinline__ T evaluate(bool need_grad, bool active) {
+        const Models<T>& m = models();
         T al[L], A[L], pc[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) al[l] = Q.from(tr[l], 3);
@@ -229,14 +306,14 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
             const T Al = T(m.X[l]) * av * dd + T(m.Y[l]) * av * (T(1) - dd) + T(m.Z[l]) * dd * (T(1) - av);
             A[l] = Al;
             const T s = tr[l], c = pc[l - 1];
-            const T pre = blend(l, s, c) * av * dd + T(m.Y[l]) * av * (T(1) - dd) * s +
+            const T pre = blend(m, l, s, c) * av * dd + T(m.Y[l]) * av * (T(1) - dd) * s +
                           T(m.Z[l]) * dd * (T(1) - av) * c;
             pc[l] = Al > T(1e-12) ? qdiv(pre, Al) : pre;
         }
         T energy = T(0), asum = T(0);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const T mine = colour ? tr[l] - mean_of(l) : T(0);
+            const T mine = colour ? tr[l] - mean_of(m, l) : T(0);
             const T d0 = Q.from(mine, 0), d1 = Q.from(mine, 1), d2 = Q.from(mine, 2);
             const T* P = m.prec[l];
             const T v0 = P[0] * d0 + P[1] * d1 + P[2] * d2;
@@ -277,15 +354,15 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         Q.sum2(terms, norm);
         const T value = energy + terms;
         if (active) {
-            ++n_values;
-            if (need_grad) ++n_gradients;
+            count(0);
+            if (need_grad) count(1);
             const bool feasible = norm < tol2;
             if (finite_(energy) && finite_(norm) &&
                 (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
                  (!feasible && best_norm >= tol2 && norm < best_norm))) {
                 have_best = true; best_norm = norm; best_energy = energy;
 #pragma unroll
-                for (int l = 0; l < L; ++l) best[l] = tr[l];
+                for (int l = 0; l < L; ++l) best(l) = tr[l];
             }
         }
         if (need_grad) {
@@ -305,7 +382,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
                 if (colour) {
                     const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
-                    blend3(l, s, c, fv, fs, fd);
+                    blend3(m, l, s, c, fv, fs, fd);
                     const T ds = av * dd * fs + Y * av * (T(1) - dd);
                     const T dc = av * dd * fd + Z * dd * (T(1) - av);
                     const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
@@ -347,7 +424,15 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     }
 
     // Two-loop recursion on the current free set; d holds q on entry/exit.
+    // Register history: unrolled over the pairs. Shared history: one trip
+    // per pair, the coefficients kept in the lane's slice (same arithmetic
+    // in the same order).
     __device__ __forceinline__ void two_loop(const bool* freev) {
+        if constexpr (HSMEM) two_loop_rolled(freev);
+        else two_loop_unrolled(freev);
+    }
+
+    __device__ __forceinline__ void two_loop_unrolled(const bool* freev) {
         T coeff[kHistory], inv[kHistory];
         T scaling = T(1);
         bool have_scaling = false;
@@ -390,21 +475,64 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         }
     }
 
-    // Starting point `s` (augmented_lagrangian.cuh:243-263); ends ready to
-    // evaluate the first outer step.
-    __device__ __forceinline__ void begin_start(int s) {
-        start = s;
+    __device__ __forceinline__ void two_loop_rolled(const bool* freev) {
+        T scaling = T(1);
+        bool have_scaling = false;
+        T* coeffs = &Slice::value(Slice::kCoeff);   // coefficient j at [2j], inverse at [2j+1] (times the stride)
+#pragma unroll 1
+        for (int j = 0; j < valid; ++j) {
+            const T* h = hist.row(j);
+            T dot = T(0), sy = T(0), ss = T(0), yy = T(0);
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (freev[l]) {
+                    const T sa = h[2 * l * kSliceStride], yb = h[(2 * l + 1) * kSliceStride];
+                    dot += sa * d[l]; sy += sa * yb; ss += sa * sa; yy += yb * yb;
+                }
+            Q.sum4(dot, sy, ss, yy);
+            const T r = qdiv(T(1), sy);
+            const T inv = (curvature_ok(sy, ss, yy) && finite_(r)) ? r : T(0);
+            const T coeff = dot * inv;
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (freev[l]) d[l] -= coeff * h[(2 * l + 1) * kSliceStride];
+            if (!have_scaling && inv > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
+            coeffs[2 * j * kSliceStride] = coeff;
+            coeffs[(2 * j + 1) * kSliceStride] = inv;
+        }
+        scaling = fmax(T(1e-12), fmin(T(1e3), scaling));
+#pragma unroll
+        for (int l = 0; l < L; ++l) d[l] *= scaling;
+#pragma unroll 1
+        for (int j = valid - 1; j >= 0; --j) {
+            const T* h = hist.row(j);
+            T dot = T(0);
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (freev[l]) dot += h[(2 * l + 1) * kSliceStride] * d[l];
+            dot = Q.sum(dot);
+            const T c = coeffs[2 * j * kSliceStride] - dot * coeffs[(2 * j + 1) * kSliceStride];
+#pragma unroll
+            for (int l = 0; l < L; ++l)
+                if (freev[l]) d[l] += c * h[2 * l * kSliceStride];
+        }
+    }
+
+    // Starting point `start` (augmented_lagrangian.cuh:243-263).
+    __device__ __forceinline__ int begin_start() {
+        const Models<T>& m = models();
+        const int s = start;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            T v = init[l];
+            T v = init(l);
             if (!REFINE && s == 1) {
                 if (!colour) v = l == 0 ? T(1) : T(0);
-                else v = l == 0 ? fmin(T(1), fmax(T(0), target)) : mean_of(l);
+                else v = l == 0 ? fmin(T(1), fmax(T(0), target)) : mean_of(m, l);
             }
-            if (REFINE && s && colour) v = mean_of(l);
+            if (REFINE && s && colour) v = mean_of(m, l);
             if (s == 2) {
-                if (!colour) v = REFINE ? init[l] : T(0.5);
-                else v = fmax(T(0.05), fmin(T(0.95), mean_of(l)));
+                if (!colour) v = REFINE ? init(l) : T(0.5);
+                else v = fmax(T(0.05), fmin(T(0.95), mean_of(m, l)));
             }
             x[l] = clampb(l, v);
         }
@@ -424,7 +552,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
                     if (dest >= T(0) && dest <= T(1) && m.mode[l] == 7) sv = fmax(sv, fmin(T(1), T(1) - dest + T(0.05)));
                     sv = clampb(l, sv);
                     x[l] = sv;
-                    const T pre = blend_value<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
+                    const T pre = blend_value_cold<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
                                   T(m.Z[l]) * da * (T(1) - al) * dest;
                     dest = Al > T(1e-12) ? pre / Al : pre;
                 }
@@ -435,14 +563,15 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         for (int r = 0; r < R; ++r) lam[r] = T(0);
         rho = T(100);
         outer = 0;
-        begin_outer();
+        return aBeginOuter;
     }
 
-    __device__ __forceinline__ void begin_outer() {
-        ++n_outer;
+    __device__ __forceinline__ int begin_outer() {
+        count(4);
 #pragma unroll
-        for (int l = 0; l < L; ++l) { ox[l] = x[l]; tr[l] = x[l]; }
+        for (int l = 0; l < L; ++l) { ox(l) = x[l]; tr[l] = x[l]; }
         phase = kOuterEval;
+        return aEval;
     }
 
     __device__ __forceinline__ T own_norm(const T* r) const {
@@ -454,9 +583,8 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     }
 
     // End of an outer step: multiplier and penalty update from the residual
-    // at x, then the next outer step, the next start, or done (phase kIdle
-    // with have_best set: the caller writes the pixel).
-    __device__ __forceinline__ void end_outer() {
+    // at x, then the next outer step, the next start, or the pixel's result.
+    __device__ __forceinline__ int end_outer() {
         const T norm = Q.sum(own_norm(resx));
         const bool feasible = norm < tol2;
 #pragma unroll
@@ -464,46 +592,45 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         if (norm > T(0.0625) * oldnorm) rho *= T(10);
         T motion = T(0);
 #pragma unroll
-        for (int l = 0; l < L; ++l) { const T dl = x[l] - ox[l]; motion += dl * dl; }
+        for (int l = 0; l < L; ++l) { const T dl = x[l] - ox(l); motion += dl * dl; }
         motion = Q.sum(motion);
         if (!(motion < tol2 && feasible) && outer + 1 < ctl.outer) {
             ++outer;
-            begin_outer();
-        } else if (start + 1 < ctl.starts) {
-            begin_start(start + 1);
-        } else {
-            phase = kIdle;
+            return aBeginOuter;
         }
+        if (start + 1 < ctl.starts) {
+            ++start;
+            return aBeginStart;
+        }
+        return aFinish;
     }
 
-    // Finds the next line-search trial point with non-zero motion (phase
-    // kTrial), or ends the inner solve when both attempts are exhausted.
-    __device__ __forceinline__ void next_trial() {
-        for (;;) {
-            if (bt < 32) {
-                T sl = T(0), mo = T(0);
+    // Next line-search trial point with non-zero motion (phase kTrial), the
+    // steepest-descent retry, or the end of the inner solve when both
+    // attempts are exhausted.
+    __device__ __forceinline__ int next_trial() {
+        if (bt < 32) {
+            T sl = T(0), mo = T(0);
 #pragma unroll
-                for (int l = 0; l < L; ++l) {
-                    tr[l] = clampb(l, x[l] + step * d[l]);
-                    const T delta = tr[l] - x[l];
-                    sl += g[l] * delta;
-                    mo += delta * delta;
-                }
-                Q.sum2(sl, mo);
-                if (mo != T(0)) { slope = sl; phase = kTrial; return; }
+            for (int l = 0; l < L; ++l) {
+                tr[l] = clampb(l, x[l] + step * d[l]);
+                const T delta = tr[l] - x[l];
+                sl += g[l] * delta;
+                mo += delta * delta;
             }
-            // This attempt failed: restart from steepest descent once.
-            valid = 0; hist.reset(); steepest();
-            if (attempt == 0) { attempt = 1; bt = 0; step = T(1); continue; }
-            end_outer();
-            return;
+            Q.sum2(sl, mo);
+            if (mo != T(0)) { slope = sl; phase = kTrial; return aEval; }
         }
+        // This attempt failed: restart from steepest descent once.
+        valid = 0; hist.reset(); steepest();
+        if (attempt == 0) { attempt = 1; bt = 0; step = T(1); return aNextTrial; }
+        return aEndOuter;
     }
 
     // Top of an inner iteration: projected gradient test, two-loop
     // direction, first trial.
-    __device__ __forceinline__ void begin_iteration() {
-        ++n_iterations;
+    __device__ __forceinline__ int begin_iteration() {
+        count(2);
         bool freev[L];
         T pg2 = T(0);
 #pragma unroll
@@ -513,7 +640,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
             pg2 += d[l] * d[l];
         }
         pg2 = Q.sum(pg2);
-        if (pg2 < T(1e-16) || !finite_(f)) { end_outer(); return; }
+        if (pg2 < T(1e-16) || !finite_(f)) return aEndOuter;
         two_loop(freev);
         T descent = T(0);
 #pragma unroll
@@ -527,11 +654,12 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         descent = Q.sum(descent);
         if (!(descent < T(0))) { valid = 0; hist.reset(); steepest(); }
         attempt = 0; bt = 0; step = T(1);
-        next_trial();
+        return aNextTrial;
     }
 
-    // Accepted step: curvature pair, move, inner termination test.
-    __device__ __forceinline__ void accept(T cand) {
+    // Accepted step (value `cand`, gradient ng): curvature pair, move, inner
+    // termination test.
+    __device__ __forceinline__ int accept() {
         T sy = T(0), ss = T(0), yy = T(0), mm = T(0);
         T sv[L], yv[L];
 #pragma unroll
@@ -554,91 +682,126 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
 #pragma unroll
         for (int q = 0; q < R; ++q) resx[q] = res[q];
         f = cand;
-        if (delta < itol * size || mm < itol) { end_outer(); return; }
-        if (++it >= ctl.inner) { end_outer(); return; }
-        begin_iteration();
+        if (delta < itol * size || mm < itol) return aEndOuter;
+        if (++it >= ctl.inner) return aEndOuter;
+        return aBeginIter;
+    }
+
+    // Decision after an evaluation, by phase.
+    __device__ __forceinline__ int after_evaluation(T value, bool need_grad) {
+        if (phase == kOuterEval) {
+            f = value;
+#pragma unroll
+            for (int l = 0; l < L; ++l) g[l] = ng[l];
+#pragma unroll
+            for (int q = 0; q < R; ++q) resx[q] = res[q];
+            oldnorm = Q.sum(own_norm(res));
+            valid = 0; hist.reset(); it = 0;
+            return aBeginIter;
+        }
+        if (phase == kTrial) {
+            count(3);
+            if (slope < T(0) && finite_(value) && value <= f + T(1e-4) * slope) {
+                if (need_grad) { cand = value; return aAccept; }
+                phase = kAcceptGrad;
+                return aEval;
+            }
+            step *= T(0.5);
+            ++bt;
+            return aNextTrial;
+        }
+        cand = value;   // kAcceptGrad
+        return aAccept;
     }
 
     // ------------------------------------------------------------ pixels --
-    // Loads pixel `i` and prepares start 0.
-    __device__ __forceinline__ void load(size_t i) {
-        const size_t n = npix;
+    // Loads pixel `i`: targets, bounds and the start-0 seed.
+    __device__ __forceinline__ void load(int i) {
+        const Models<T>& m = models();
+        const size_t n = pixels();
         pixel = i;
-        target64 = colour ? img[3 * i + Q.q] : 0.0;
-        target = T(target64);
-        bg64 = (REFINE && smooth && colour) ? a.targets[(size_t(L) + Q.q) * n + i] : 0.0;
-        bgq = T(bg64);
+        target = T(colour ? image()[3 * size_t(i) + Q.q] : 0.0);
+        bgq = T((REFINE && smooth && colour) ? a.targets[(size_t(L) + Q.q) * n + i] : 0.0);
 #pragma unroll
         for (int l = 0; l < R; ++l) {
             double t = REFINE ? a.targets[size_t(l) * n + i] : 0.0;
             if (REFINE && opaque && l == 0) t = 1.0;
             ahat[l] = T(t);
         }
+        const float* wp = REFINE ? nullptr : warm();
 #pragma unroll
         for (int l = 0; l < L; ++l) {
+            T v;
             if (colour) {
-                if (REFINE) init[l] = (smooth && l == 0) ? bgq : T(a.first[(size_t(l) * n + i) * 4 + Q.q]);
-                else init[l] = fmin(T(1), fmax(T(0), mean_of(l)));
+                if (REFINE) v = (smooth && l == 0) ? bgq : T(a.first[(size_t(l) * n + i) * 4 + Q.q]);
+                else v = fmin(T(1), fmax(T(0), mean_of(m, l)));
             } else {
-                init[l] = (opaque && l == 0) ? T(1) : (REFINE ? ahat[REFINE ? l : 0] : T(0.5));
+                v = (opaque && l == 0) ? T(1) : (REFINE ? ahat[REFINE ? l : 0] : T(0.5));
             }
             if (!REFINE && wp) {
                 // Learned warm start: the network's prediction replaces the
                 // start-0 seed (bounds still apply when the start is seeded).
-                const float* wv = wp + i * size_t(4 * L);
-                init[l] = T(colour ? wv[L + 3 * l + Q.q] : wv[l]);
+                const float* wv = wp + size_t(i) * size_t(4 * L);
+                v = T(colour ? wv[L + 3 * l + Q.q] : wv[l]);
             }
+            init(l) = v;
         }
         have_best = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);
-        n_values = n_gradients = n_iterations = n_backtracks = n_outer = 0;
-        begin_start(0);
+        if (a.counters)
+#pragma unroll
+            for (int k = 0; k < Slice::kCounters; ++k) counter(k) = 0;
     }
 
     // Writes the finished pixel: output (pinned values exactly), FP64
     // feasibility check, status, miss list, counters.
-    __device__ __forceinline__ void store(bool skipped) {
-        const size_t n = npix, i = pixel;
-        double v[L], ah[R];
-#pragma unroll
-        for (int l = 0; l < R; ++l) {
-            double t = REFINE ? a.targets[size_t(l) * n + i] : 0.0;
-            if (REFINE && opaque && l == 0) t = 1.0;
-            ah[l] = t;
-        }
+    __device__ void store(bool skipped) {
+        const Models<T>& m = models();
+        const size_t n = pixels(), i = size_t(pixel);
+        double* outp = output();
+        double v0 = 0.0;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            v[l] = double(have_best ? best[l] : init[l]);
-            if (REFINE && !colour) v[l] = ah[REFINE ? l : 0];
-            if (REFINE && smooth && colour && l == 0) v[l] = bg64;
-            if (!REFINE && opaque && !colour && l == 0) v[l] = 1.0;
-            outp[(size_t(l) * n + i) * 4 + Q.q] = v[l];
+            double v = double(have_best ? best(l) : init(l));
+            if (REFINE && !colour) v = (opaque && l == 0) ? 1.0 : a.targets[size_t(l) * n + i];
+            if (REFINE && smooth && colour && l == 0) v = a.targets[(size_t(L) + Q.q) * n + i];
+            if (!REFINE && opaque && !colour && l == 0) v = 1.0;
+            outp[(size_t(l) * n + i) * 4 + Q.q] = v;
+            if (l == 0) v0 = v;
         }
-        // FP64 constraint check of the written point (solver_workspace.cuh:18-38).
-        double av[L];
-#pragma unroll
-        for (int l = 0; l < L; ++l) av[l] = Q.from(v[l], 3);
-        double A = av[0], c = v[0];
-#pragma unroll
+        // FP64 constraint check of the written point (solver_workspace.cuh:18-38),
+        // one layer per trip, reading back the values just written.
+        double A = Q.from(v0, 3), c = v0;
+#pragma unroll 1
         for (int l = 1; l < L; ++l) {
-            const double al = av[l], dd = A;
+            const double s = outp[(size_t(l) * n + i) * 4 + Q.q];
+            const double al = Q.from(s, 3), dd = A;
             const double Al = double(m.X[l]) * al * dd + double(m.Y[l]) * al * (1.0 - dd) +
                               double(m.Z[l]) * dd * (1.0 - al);
-            const double s = v[l];
             const double pre = blend_value<double>(m.mode[l], s, c) * al * dd + double(m.Y[l]) * al * (1.0 - dd) * s +
                                double(m.Z[l]) * dd * (1.0 - al) * c;
             c = Al > 1e-12 ? pre / Al : pre;
             A = Al;
         }
         double norm = 0.0;
-        if (colour) { const double r = c - target64; norm = r * r; }
-        else if (REFINE) {
-#pragma unroll
-            for (int l = 0; l < R; ++l) { const double r = v[l] - ah[l]; norm += r * r; }
-        } else { const double r = A - 1.0; norm = r * r; }
+        if (colour) {
+            const double r = c - image()[3 * i + Q.q];
+            norm = r * r;
+        } else if (REFINE) {
+#pragma unroll 1
+            for (int l = 0; l < R; ++l) {
+                const double t = (opaque && l == 0) ? 1.0 : a.targets[size_t(l) * n + i];
+                const double r = outp[(size_t(l) * n + i) * 4 + 3] - t;
+                norm += r * r;
+            }
+        } else {
+            const double r = A - 1.0;
+            norm = r * r;
+        }
         norm = Q.sum(norm);
         const bool miss = !(norm < ctl.outer_tolerance * ctl.outer_tolerance);
         if (Q.q == 0) {
+            int32_t* stp = status();
             if (skipped) {
                 if (stp) stp[i] = 8;
                 if (a.input_failed) atomicAdd(a.input_failed, 1);
@@ -647,92 +810,74 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
                 if (miss && a.miss_list) a.miss_list[atomicAdd(a.miss_count, 1)] = int32_t(gidx);
             }
             if (a.counters) {
-                uint32_t* cnt = a.counters + 5 * gidx;
-                cnt[0] = n_values; cnt[1] = n_gradients; cnt[2] = n_iterations; cnt[3] = n_backtracks; cnt[4] = n_outer;
+                uint32_t* out = a.counters + 5 * size_t(gidx);
+#pragma unroll
+                for (int k = 0; k < Slice::kCounters; ++k) out[k] = counter(k);
             }
         }
     }
 
-    // Pulls pixels until one needs solving (phase != kIdle) or the queue is
-    // empty (phase kIdle, returns false).
-    __device__ __forceinline__ bool fetch(int total) {
-        for (;;) {
-            int job = 0;
-            if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
-            job = Q.from(job, 0);
-            if (job >= total) { phase = kIdle; return false; }
-            gidx = size_t(a.list ? a.list[job] : job);
-            size_t i = gidx;
-            if (BATCH) {
-                // The image owning queue index gidx: last job with offset <= gidx.
-                int lo = 0, hi = a.job_count - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (a.jobs[mid].offset <= int64_t(gidx)) lo = mid; else hi = mid - 1;
-                }
-                const BatchJob& J = a.jobs[lo];
-                if (lo != job_id) {
-                    // Stage this image's layer models in the quad's slot (a
-                    // typed copy: the solver reads the fields with their types).
-                    __syncwarp(Q.mask);
-                    if (Q.q == 0) const_cast<Models<T>&>(m) = static_cast<const Models<T>*>(a.models)[J.model];
-                    __syncwarp(Q.mask);
-                    job_id = lo;
-                }
-                img = J.image; outp = J.out; stp = J.status; wp = J.warm; npix = size_t(J.n);
-                i = gidx - size_t(J.offset);
-            } else {
-                img = a.image; outp = a.out; stp = a.status; wp = a.warm; npix = size_t(a.n);
+    // Pulls the next pixel: aBeginStart when it needs solving, aFetch again
+    // after a pixel that is written without solving, aEval with `live`
+    // cleared when the queue is empty.
+    __device__ int fetch(int total, bool& live) {
+        int job = 0;
+        if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
+        job = Q.from(job, 0);
+        if (job >= total) { phase = kIdle; live = false; return aEval; }
+        gidx = a.list ? a.list[job] : job;
+        int i = gidx;
+        if constexpr (BATCH) {
+            // The image owning queue index gidx: last job with offset <= gidx.
+            int lo = 0, hi = a.job_count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (a.jobs[mid].offset <= int64_t(gidx)) lo = mid; else hi = mid - 1;
             }
-            load(i);
-            if (REFINE && a.input_status && a.input_status[i] != 0) {
-                // Targets that cannot be normalized: keep the initial layers
-                // and report status 8 (solver_workspace.cuh:144).
-                have_best = false;
-                n_values = n_gradients = n_iterations = n_backtracks = n_outer = 0;
-                store(true);
-                continue;
+            if (lo != job_id) {
+                // Stage this image's layer models in the quad's slot (a typed
+                // copy: the solver reads the fields with their types).
+                __syncwarp(Q.mask);
+                if (Q.q == 0) const_cast<Models<T>&>(models()) = static_cast<const Models<T>*>(a.models)[a.jobs[lo].model];
+                __syncwarp(Q.mask);
+                job_id = lo;
             }
-            return true;
+            i = gidx - int(a.jobs[lo].offset);
         }
+        load(i);
+        if (REFINE && a.input_status && a.input_status[i] != 0) {
+            // Targets that cannot be normalized: keep the initial layers and
+            // report status 8 (solver_workspace.cuh:144).
+            store(true);
+            return aFetch;
+        }
+        start = 0;
+        return aBeginStart;
     }
 
     // ------------------------------------------------------------- loop --
     __device__ void run() {
         const int total = a.list ? *a.list_count : a.n;
-        bool live = fetch(total);
+        bool live = true;
+        int act = aFetch;
         for (;;) {
+            while (act != aEval) {
+                switch (act) {
+                case aBeginIter: act = begin_iteration(); break;
+                case aNextTrial: act = next_trial(); break;
+                case aAccept: act = accept(); break;
+                case aEndOuter: act = end_outer(); break;
+                case aBeginStart: act = begin_start(); break;
+                case aBeginOuter: act = begin_outer(); break;
+                case aFinish: store(false); act = aFetch; break;
+                default: act = fetch(total, live); break;
+                }
+            }
             if (__all_sync(0xffffffffu, !live)) break;
             const bool need_grad = phase == kOuterEval || phase == kAcceptGrad ||
                                    (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial);
             const T value = evaluate(need_grad && live, live);
-            if (!live) continue;
-            if (phase == kOuterEval) {
-                f = value;
-#pragma unroll
-                for (int l = 0; l < L; ++l) g[l] = ng[l];
-#pragma unroll
-                for (int q = 0; q < R; ++q) resx[q] = res[q];
-                oldnorm = Q.sum(own_norm(res));
-                valid = 0; hist.reset(); it = 0;
-                begin_iteration();
-            } else if (phase == kTrial) {
-                ++n_backtracks;
-                if (slope < T(0) && finite_(value) && value <= f + T(1e-4) * slope) {
-                    if (need_grad) accept(value);
-                    else phase = kAcceptGrad;
-                } else {
-                    step *= T(0.5);
-                    ++bt;
-                    next_trial();
-                }
-            } else {   // kAcceptGrad
-                accept(value);
-            }
-            if (phase == kIdle) {
-                store(false);
-                live = fetch(total);
-            }
+            act = live ? after_evaluation(value, need_grad) : aEval;
         }
     }
 };

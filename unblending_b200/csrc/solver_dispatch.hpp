@@ -8,17 +8,53 @@ namespace unb {
 
 // Persistent solve over SolveArgs::n pixels (or SolveArgs::list); the grid
 // is `threads`-wide blocks times the occupancy limit times `sms`.
-// variant 0: L-BFGS history in registers; 1: in shared memory.
+// FP32 variants: 0 L-BFGS history in registers; 1, 2, 3, 4 history in shared
+// memory with registers capped for 4, 3, 5, 6 blocks of 128 threads per SM.
+// FP64 variants (history always in shared memory): 0 uncapped registers;
+// 1, 2 capped for 2, 3 blocks per SM.
+constexpr int kFp32Variants = 5, kFp64Variants = 3;
 cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<float>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
-cudaError_t launch_solve_fp64(int L, bool refine, const Models<double>& m, const SolverControls& c,
+cudaError_t launch_solve_fp64(int L, bool refine, int variant, const Models<double>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
 // Batched first pass over the images of one layer-count group
-// (SolveArgs::jobs / models); variant 0 or 2 as above.
+// (SolveArgs::jobs / models); variants as above.
 cudaError_t launch_solve_batch_fp32(int L, int variant, const SolverControls& c, const SolveArgs& a, int threads,
                                     int sms, cudaStream_t s);
-cudaError_t launch_solve_batch_fp64(int L, const SolverControls& c, const SolveArgs& a, int threads, int sms,
-                                    cudaStream_t s);
+cudaError_t launch_solve_batch_fp64(int L, int variant, const SolverControls& c, const SolveArgs& a, int threads,
+                                    int sms, cudaStream_t s);
+
+// The same per layer count: one translation unit per layer count
+// (solver_l<L>.cu) defines these specializations, so the counts compile in
+// parallel.
+template <int L> cudaError_t solve_fp32_layers(bool refine, int variant, const Models<float>& m,
+                                               const SolverControls& c, const SolveArgs& a, int threads, int sms,
+                                               cudaStream_t s);
+template <int L> cudaError_t solve_fp64_layers(bool refine, int variant, const Models<double>& m,
+                                               const SolverControls& c, const SolveArgs& a, int threads, int sms,
+                                               cudaStream_t s);
+template <int L> cudaError_t solve_batch_fp32_layers(int variant, const SolverControls& c, const SolveArgs& a,
+                                                     int threads, int sms, cudaStream_t s);
+template <int L> cudaError_t solve_batch_fp64_layers(int variant, const SolverControls& c, const SolveArgs& a,
+                                                     int threads, int sms, cudaStream_t s);
+#define UNB_DECLARE_LAYER_SOLVES(L)                                                                              \
+    template <> cudaError_t solve_fp32_layers<L>(bool, int, const Models<float>&, const SolverControls&,         \
+                                                 const SolveArgs&, int, int, cudaStream_t);                      \
+    template <> cudaError_t solve_fp64_layers<L>(bool, int, const Models<double>&, const SolverControls&,        \
+                                                 const SolveArgs&, int, int, cudaStream_t);                      \
+    template <> cudaError_t solve_batch_fp32_layers<L>(int, const SolverControls&, const SolveArgs&, int, int,   \
+                                                       cudaStream_t);                                            \
+    template <> cudaError_t solve_batch_fp64_layers<L>(int, const SolverControls&, const SolveArgs&, int, int,   \
+                                                       cudaStream_t);
+UNB_DECLARE_LAYER_SOLVES(1)
+UNB_DECLARE_LAYER_SOLVES(2)
+UNB_DECLARE_LAYER_SOLVES(3)
+UNB_DECLARE_LAYER_SOLVES(4)
+UNB_DECLARE_LAYER_SOLVES(5)
+UNB_DECLARE_LAYER_SOLVES(6)
+UNB_DECLARE_LAYER_SOLVES(7)
+UNB_DECLARE_LAYER_SOLVES(8)
+#undef UNB_DECLARE_LAYER_SOLVES
 
 // Guided-filter refinement targets, FP64 throughout.
 struct FilterArgs {

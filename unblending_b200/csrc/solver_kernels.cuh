@@ -6,15 +6,13 @@
 
 namespace unb {
 
-// Dynamic shared memory: the L-BFGS history (HSMEM), then one layer-model
-// slot per quad (BATCH).
+// Dynamic shared memory: every lane's slice (cold values, the L-BFGS
+// history when HSMEM, work counters), then one layer-model slot per quad
+// (BATCH).
 template <class T, int L, bool HSMEM, bool BATCH> struct SolveSmem {
-    __host__ __device__ static size_t history(int threads) {
-        return HSMEM ? size_t(threads) * kHistory * L * 2 * sizeof(T) : 0;
-    }
+    using Slice = LaneSlice<T, L, HSMEM>;
     static size_t bytes(int threads) {
-        const size_t h = (history(threads) + 15) / 16 * 16;
-        return h + (BATCH ? size_t(threads / 4) * sizeof(Models<T>) : 0);
+        return Slice::bytes() + (BATCH ? size_t(threads / 4) * sizeof(Models<T>) : 0);
     }
 };
 
@@ -23,18 +21,8 @@ template <class T, int L, bool REFINE, bool HSMEM, int MINB, bool BATCH>
 __global__ void __launch_bounds__(128, MINB)
 solve_pixels(const __grid_constant__ Models<T> m, const __grid_constant__ SolverControls ctl,
              const __grid_constant__ SolveArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    if constexpr (BATCH) {
-        const size_t h = (SolveSmem<T, L, HSMEM, BATCH>::history(blockDim.x) + 15) / 16 * 16;
-        Models<T>* slots = reinterpret_cast<Models<T>*>(smem_raw + h);
-        QuadSolver<T, L, REFINE, HSMEM, true> S(slots[threadIdx.x >> 2], ctl, a);
-        S.hist.init(reinterpret_cast<T*>(smem_raw));
-        S.run();
-    } else {
-        QuadSolver<T, L, REFINE, HSMEM, false> S(m, ctl, a);
-        S.hist.init(reinterpret_cast<T*>(smem_raw));
-        S.run();
-    }
+    QuadSolver<T, L, REFINE, HSMEM, BATCH> S(&m, ctl, a);
+    S.run();
 }
 
 template <class T, int L, bool REFINE, bool HSMEM, int MINB = 1, bool BATCH = false> struct SolveLauncher {

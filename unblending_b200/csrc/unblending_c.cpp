@@ -217,18 +217,22 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
         (out.resolve_misses != 0 && out.resolve_misses != 1) ||
         (out.threads_per_block != 0 && (out.threads_per_block % 32 != 0 || out.threads_per_block < 32 ||
                                         out.threads_per_block > 128)) ||
-        out.kernel_variant < -1 || out.kernel_variant > 2)
+        out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
+        out.fp64_variant >= kFp64Variants)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
 
-// FP32 kernel variant measured on B200 (1024x1024, 5 layers): the first pass
-// is faster with the L-BFGS history in registers (226 vs 339 ms), the
-// refinement with it in shared memory (192 vs 203 ms).
+// FP32 kernel variant measured on B200 (1024x1024, 5 layers, FP32 solve
+// times of the first pass / refinement in ms): history in registers 202 / 195,
+// shared history with 4 blocks per SM 194 / 158, 3 blocks 220 / 178,
+// 5 blocks 199 / 173, 6 blocks 205 / 220.
 int default_fp32_variant(int L, bool refine) {
-    (void)L;
-    return refine ? 1 : 0;
+    (void)L; (void)refine;
+    return 1;
 }
+
+int fp64_variant(const unblending_solver_options& so) { return so.fp64_variant >= 0 ? so.fp64_variant : 0; }
 
 template <class T> Models<T> make_models(const unblending_layer* layers, int L) {
     Models<T> m{};
@@ -359,7 +363,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     }
     const int threads = so.threads_per_block ? so.threads_per_block : 128;
     if (so.precision == UNBLENDING_PRECISION_FP64) {
-        ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, a, threads, c.sms, s));
+        ck(launch_solve_fp64(L, refine, fp64_variant(so), make_models<double>(layers, L), ctl, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
         ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -376,7 +380,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
             b.queue = queues + 1;
             b.input_status = nullptr; b.input_failed = nullptr;
             b.warm = nullptr;   // misses fall back to the reference's (cold) start
-            ck(launch_solve_fp64(L, refine, make_models<double>(layers, L), ctl, b, threads, c.sms, s));
+            ck(launch_solve_fp64(L, refine, fp64_variant(so), make_models<double>(layers, L), ctl, b, threads, c.sms, s));
             ++t_launches;
         } else {
             ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -749,7 +753,6 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 } else {
                     G.variant = so.kernel_variant >= 0 ? so.kernel_variant : 0;
                     G.threads = so.threads_per_block ? so.threads_per_block : 128;
-                    if (G.variant == 1) G.variant = 2;   // batch kernels: register or 3-block shared history
                 }
                 gs.push_back(G);
             }
@@ -766,13 +769,13 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                         ++launches;
                     }
                     if (so.precision == UNBLENDING_PRECISION_FP64) {
-                        ck(launch_solve_batch_fp64(G.L, ctl, G.fp, 128, c.sms, s));
+                        ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.fp, 128, c.sms, s));
                         ++launches;
                     } else {
                         ck(launch_solve_batch_fp32(G.L, G.variant, ctl, G.fp, G.threads, c.sms, s));
                         ++launches;
                         if (so.resolve_misses) {
-                            ck(launch_solve_batch_fp64(G.L, ctl, G.re, 128, c.sms, s));
+                            ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.re, 128, c.sms, s));
                             ++launches;
                         } else {
                             ck(cudaMemcpyAsync(G.counts + 1, G.counts, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -1069,7 +1072,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
         a.miss_count = counts + 0;
         const int threads = so.threads_per_block ? so.threads_per_block : 128;
         if (so.precision == UNBLENDING_PRECISION_FP64) {
-            ck(launch_solve_fp64(L, false, make_models<double>(layers, L), ctl, a, threads, sms, s));
+            ck(launch_solve_fp64(L, false, fp64_variant(so), make_models<double>(layers, L), ctl, a, threads, sms, s));
             ++t_launches;
         } else {
             const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
@@ -1080,7 +1083,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
                 b.list = list_a; b.list_count = counts + 0;
                 b.miss_list = list_b; b.miss_count = counts + 1;
                 b.queue = queues + 1;
-                ck(launch_solve_fp64(L, false, make_models<double>(layers, L), ctl, b, threads, sms, s));
+                ck(launch_solve_fp64(L, false, fp64_variant(so), make_models<double>(layers, L), ctl, b, threads, sms, s));
                 ++t_launches;
             }
         }
