@@ -43,10 +43,12 @@ typedef struct unblending_solver_options {
     const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start */
     int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default, 0 uncapped registers, 1/2 capped for
                                    2/3 blocks per SM */
+    int32_t fp32_outer;         /* FP32 precision with resolve_misses: outer steps of the FP32 solve before a
+                                   pixel is left to the FP64 re-solve (default 12; 0 = outer) */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 12 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

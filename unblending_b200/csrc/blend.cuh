@@ -113,9 +113,14 @@ template <class T> __device__ __forceinline__ T qdiv(T a, T b);
 template <> __device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
 template <> __device__ __forceinline__ double qdiv<double>(double a, double b) { return a / b; }
 
+template <class T>
+__device__ __noinline__ void blend_special(int sp, T s, T d, T& f, T& fs, T& fd, bool partials);
+
 // Table-driven blend for the FP32 solver: the ten piecewise-bilinear modes
-// without any jump (coefficients selected by a compare), Dodge/Burn/SoftLight
-// behind layer-uniform branches. Same piecewise definitions as blend_all.
+// without any jump (coefficients selected by a compare); Dodge, Burn and
+// SoftLight (a layer-uniform branch) in one out-of-line function, so that
+// their code is not copied into every unrolled layer of the solver. Same
+// piecewise definitions as blend_all.
 template <class T, class M>
 __device__ __forceinline__ void blend_table(const M& m, int l, T s, T d, T& f, T& fs, T& fd, bool partials) {
     const int sp = m.special[l];
@@ -130,6 +135,11 @@ __device__ __forceinline__ void blend_table(const M& m, int l, T s, T d, T& f, T
         if (partials) { fs = cs + csd * d; fd = cd + csd * s; }
         return;
     }
+    blend_special<T>(sp, s, d, f, fs, fd, partials);
+}
+
+template <class T>
+__device__ __noinline__ void blend_special(int sp, T s, T d, T& f, T& fs, T& fd, bool partials) {
     const T one = T(1), two = T(2), eps = T(1e-5);
     if (sp == 6) {
         const T q = one - s;

@@ -52,9 +52,11 @@ template <class T> __device__ __forceinline__ bool finite_(T v);
 template <> __device__ __forceinline__ bool finite_<float>(float v) { return isfinite(v); }
 template <> __device__ __forceinline__ bool finite_<double>(double v) { return isfinite(v); }
 
-// Blend value on cold paths (the third start's seeding), kept out of line so
-// that its switch over the modes is not copied into every unrolled layer.
-template <class T> __device__ __noinline__ T blend_value_cold(int mode, T s, T d) { return blend_value<T>(mode, s, d); }
+// The FP64 blend functions (a switch over the thirteen modes) out of line:
+// one copy of each serves every unrolled layer, which keeps the solver's loop
+// small for the instruction cache. The FP32 solver uses blend_table.
+template <class T> __device__ __noinline__ T blend_value_call(int mode, T s, T d) { return blend_value<T>(mode, s, d); }
+template <class T> __device__ __noinline__ void blend_all_call(int mode, T s, T d, T& f, T& fs, T& fd) { blend_all<T>(mode, s, d, f, fs, fd); }
 
 // Dynamic shared memory of the solve kernels (one declaration for all of
 // them; addressed by thread index, so no pointer stays live in registers).
@@ -276,11 +278,11 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     static constexpr bool kFast = sizeof(T) == 4;
     __device__ __forceinline__ T blend(const Models<T>& m, int l, T s, T d) const {
         if constexpr (kFast) { T f, fs, fd; blend_table<T>(m, l, s, d, f, fs, fd, false); return f; }
-        else return blend_value<T>(m.mode[l], s, d);
+        else return blend_value_call<T>(m.mode[l], s, d);
     }
     __device__ __forceinline__ void blend3(const Models<T>& m, int l, T s, T d, T& f, T& fs, T& fd) const {
         if constexpr (kFast) blend_table<T>(m, l, s, d, f, fs, fd, true);
-        else blend_all<T>(m.mode[l], s, d, f, fs, fd);
+        else blend_all_call<T>(m.mode[l], s, d, f, fs, fd);
     }
 
     // sy > 1e-9 sqrt(ss yy) and sy > 0 (augmented_lagrangian.cuh:193,290); the
@@ -552,7 +554,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
                     if (dest >= T(0) && dest <= T(1) && m.mode[l] == 7) sv = fmax(sv, fmin(T(1), T(1) - dest + T(0.05)));
                     sv = clampb(l, sv);
                     x[l] = sv;
-                    const T pre = blend_value_cold<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
+                    const T pre = blend_value_call<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
                                   T(m.Z[l]) * da * (T(1) - al) * dest;
                     dest = Al > T(1e-12) ? pre / Al : pre;
                 }

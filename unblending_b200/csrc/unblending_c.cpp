@@ -218,7 +218,7 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
         (out.threads_per_block != 0 && (out.threads_per_block % 32 != 0 || out.threads_per_block < 32 ||
                                         out.threads_per_block > 128)) ||
         out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
-        out.fp64_variant >= kFp64Variants)
+        out.fp64_variant >= kFp64Variants || out.fp32_outer < 0)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -233,6 +233,23 @@ int default_fp32_variant(int L, bool refine) {
 }
 
 int fp64_variant(const unblending_solver_options& so) { return so.fp64_variant >= 0 ? so.fp64_variant : 0; }
+
+SolverControls controls(const unblending_solver_options& so) {
+    SolverControls c;
+    c.inner = so.inner; c.outer = so.outer; c.starts = so.starts;
+    c.inner_tolerance = so.inner_tolerance; c.outer_tolerance = so.outer_tolerance;
+    return c;
+}
+
+// Controls of the FP32 solve. When its misses are re-solved in FP64, the FP32
+// solve stops after fp32_outer outer steps: a pixel still unsolved by then
+// almost never converges later (it runs to the outer cap and fails), and the
+// FP64 re-solve gives it the reference method's own result anyway.
+SolverControls fp32_controls(const unblending_solver_options& so) {
+    SolverControls c = controls(so);
+    if (so.resolve_misses && so.fp32_outer > 0 && so.fp32_outer < c.outer) c.outer = so.fp32_outer;
+    return c;
+}
 
 template <class T> Models<T> make_models(const unblending_layer* layers, int L) {
     Models<T> m{};
@@ -341,9 +358,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     }
     ck(cudaEventRecord(c.ev[1], s));
 
-    SolverControls ctl;
-    ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
-    ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+    const SolverControls ctl = controls(so), ctl32 = fp32_controls(so);
     SolveArgs a;
     a.n = int(n);
     a.image = io.image; a.first = io.first; a.targets = targets; a.out = io.out;
@@ -369,7 +384,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
     } else {
         const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, refine);
-        ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl, a, threads, c.sms, s));
+        ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
         if (so.resolve_misses) {
@@ -635,9 +650,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
             c.plan.reset();
             auto plan = std::make_unique<BatchPlan>();
             plan->key = key;
-            SolverControls ctl;
-            ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
-            ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+            const SolverControls ctl = controls(so), ctl32 = fp32_controls(so);
             struct Group {
                 int L;
                 SolveArgs fp, re;      // first solve (warm where given), FP64 re-solve (reference start)
@@ -740,7 +753,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                             t.miss_list = nullptr; t.status = nullptr;
                             ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
                             ck(cudaEventRecord(c.ev[4], s));
-                            ck(launch_solve_batch_fp32(L, cand.first, ctl, t, cand.second, c.sms, s));
+                            ck(launch_solve_batch_fp32(L, cand.first, ctl32, t, cand.second, c.sms, s));
                             ck(cudaEventRecord(c.ev[5], s));
                             ck(cudaEventSynchronize(c.ev[5]));
                             const float ms = elapsed(c.ev[4], c.ev[5]);
@@ -772,7 +785,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                         ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.fp, 128, c.sms, s));
                         ++launches;
                     } else {
-                        ck(launch_solve_batch_fp32(G.L, G.variant, ctl, G.fp, G.threads, c.sms, s));
+                        ck(launch_solve_batch_fp32(G.L, G.variant, ctl32, G.fp, G.threads, c.sms, s));
                         ++launches;
                         if (so.resolve_misses) {
                             ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.re, 128, c.sms, s));
@@ -1060,9 +1073,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
         // The array keeps the previous call's contents: the queue heads and
         // counters must start at zero; the lists are written before they are read.
         ck(cudaMemsetAsync(base, 0, 64, s));
-        SolverControls ctl;
-        ctl.inner = so.inner; ctl.outer = so.outer; ctl.starts = so.starts;
-        ctl.inner_tolerance = so.inner_tolerance; ctl.outer_tolerance = so.outer_tolerance;
+        const SolverControls ctl = controls(so), ctl32 = fp32_controls(so);
         SolveArgs a;
         a.n = int(n);
         a.image = image; a.out = output; a.status = status;
@@ -1076,7 +1087,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
             ++t_launches;
         } else {
             const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
-            ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl, a, threads, sms, s));
+            ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl32, a, threads, sms, s));
             ++t_launches;
             if (so.resolve_misses) {
                 SolveArgs b = a;
