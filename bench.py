@@ -47,6 +47,10 @@ UNIT = "pixels/s"
 WORKLOAD = "rgb1024_l5"
 PEAK_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal: SMs x FP32 lanes x FMA x max clock
 SAMPLE = 4096                                        # pixels in the CPU baseline / parity sample
+# DRAM bytes (read + write) per pixel of one FP32 first-pass solve launch on this
+# workload, from an ncu capture of that kernel (dram__bytes x duration): the
+# image read and the packed-RGBA output write, no re-reads.
+SOLVE_TRAFFIC_BYTES_PER_PIXEL = 145.0
 
 
 def parse():
@@ -420,7 +424,7 @@ def b200_arm(args):
         "counters_mean": {"unmix": c1.mean(0).tolist(), "refine": c2.mean(0).tolist(),
                           "fields": ["values", "gradients", "iterations", "line_search_trials", "outer"]},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": PEAK_FP32_TFLOPS, "unit": "TFLOP/s",
-                     "frac": achieved / PEAK_FP32_TFLOPS, "traffic": None,
+                     "frac": achieved / PEAK_FP32_TFLOPS, "traffic": SOLVE_TRAFFIC_BYTES_PER_PIXEL * n,
                      "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json has no FP32 figure",
                      "flops_per_step": flops1 + flops2, "kernel": "solve_pixels<float,5,...>"},
         "roofline_filter": {"bound": "hbm", "achieved": filter_gbs, "peak": hbm_peak, "unit": "GB/s",
