@@ -38,11 +38,13 @@ typedef struct unblending_solver_options {
     double inner_tolerance;     /* default 5e-3 */
     double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
     int32_t threads_per_block;  /* 0 selects the tuned default */
-    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1..4 in shared memory
-                                   with registers capped for 4, 3, 5, 6 blocks per SM */
+    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1/2 in shared memory
+                                   with registers capped for 4/3 blocks per SM, 3/4 in global memory capped
+                                   for 5/6 blocks per SM */
     const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start */
-    int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default, 0 uncapped registers, 1/2 capped for
-                                   2/3 blocks per SM */
+    int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default; history in shared memory with 0
+                                   uncapped registers, 1/2 capped for 2/3 blocks per SM; history in global
+                                   memory with 3/4 capped for 3/4 blocks per SM */
     int32_t fp32_outer;         /* FP32 precision with resolve_misses: outer steps of the FP32 solve before a
                                    pixel is left to the FP64 re-solve (default 12; 0 = outer) */
 } unblending_solver_options;

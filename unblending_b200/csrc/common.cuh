@@ -8,6 +8,9 @@ namespace unb {
 
 constexpr int kMaxLayers = 8;       // compiled layer counts 1..8
 constexpr int kHistory = 6;         // L-BFGS memory (augmented_lagrangian.cuh:164)
+// Lane stride of the solver's per-lane storage: the largest block (128
+// threads), so that slice offsets are compile-time constants for any block size.
+constexpr int kSliceStride = 128;
 
 // Layer descriptors in the solver's arithmetic type, passed by value as a
 // kernel parameter (lives in the constant bank, no global state).
@@ -101,6 +104,10 @@ struct SolveArgs {
     int job_count = 0;
     const void* models = nullptr;
     int opaque = 1, smooth = 0;
+    // Global-memory L-BFGS history (kernels that keep it there): room for
+    // history_lanes lanes; the launch uses at most history_lanes / 128 blocks.
+    void* history = nullptr;
+    int history_lanes = 0;
 };
 
 }  // namespace unb

@@ -61,9 +61,12 @@ template <class T> __device__ __noinline__ void blend_all_call(int mode, T s, T 
 // Dynamic shared memory of the solve kernels (one declaration for all of
 // them; addressed by thread index, so no pointer stays live in registers).
 extern __shared__ __align__(16) unsigned char solver_smem[];
-// Lane stride of the per-lane slices: the largest block (128 threads), so
-// that slice offsets are compile-time constants for any block size.
-constexpr int kSliceStride = 128;
+
+// Where the L-BFGS history lives: registers (a shift register), the lane's
+// shared-memory slice, or a per-lane global-memory array (coalesced across
+// lanes, served by L1/L2), which frees shared memory for more resident
+// blocks when the values are wide (FP64).
+enum : int { kHistRegisters = 0, kHistShared = 1, kHistGlobal = 2 };
 
 struct Quad {
     unsigned mask;
@@ -106,12 +109,14 @@ struct Quad {
 // L-BFGS pairs, indexed by age j (0 = newest). Register form: a shift
 // register with compile-time indices. Shared-memory form: a ring buffer in
 // the lane's slice after its cold values, element (slot, l, s|y) at
-// slice index 3L + (slot*L + l)*2 + w.
-template <class T, int L, bool SMEM> struct History;
+// slice index 3L + (slot*L + l)*2 + w. Global form: the same ring buffer in
+// SolveArgs::history, element k of lane g at [k * lanes + g] with
+// g = blockIdx.x * kSliceStride + threadIdx.x and lanes = gridDim.x * kSliceStride.
+template <class T, int L, int HS> struct History;
 
-template <class T, int L> struct History<T, L, false> {
+template <class T, int L> struct History<T, L, kHistRegisters> {
     T s_[kHistory][L], y_[kHistory][L];
-    __device__ __forceinline__ void init() {}
+    __device__ __forceinline__ void init(void*) {}
     __device__ __forceinline__ T s(int j, int l) const { return s_[j][l]; }
     __device__ __forceinline__ T y(int j, int l) const { return y_[j][l]; }
     __device__ __forceinline__ void push(const T* sv, const T* yv) {
@@ -125,7 +130,7 @@ template <class T, int L> struct History<T, L, false> {
     __device__ __forceinline__ void reset() {}
 };
 
-template <class T, int L> struct History<T, L, true> {
+template <class T, int L> struct History<T, L, kHistShared> {
     static constexpr int kBase = 3 * L;   // after the lane slice's cold values
     int next;
     // This lane's pair of age j: element l of s at row(j)[2*l*kSliceStride],
@@ -135,7 +140,8 @@ template <class T, int L> struct History<T, L, true> {
         k = k < 0 ? k + kHistory : k;
         return reinterpret_cast<T*>(solver_smem) + (kBase + k * 2 * L) * kSliceStride + threadIdx.x;
     }
-    __device__ __forceinline__ void init() { next = 0; }
+    __device__ __forceinline__ void init(void*) { next = 0; }
+    __device__ static constexpr int stride() { return kSliceStride; }
     __device__ __forceinline__ T s(int j, int l) const { return row(j)[2 * l * kSliceStride]; }
     __device__ __forceinline__ T y(int j, int l) const { return row(j)[(2 * l + 1) * kSliceStride]; }
     __device__ __forceinline__ void push(const T* sv, const T* yv) {
@@ -150,15 +156,45 @@ template <class T, int L> struct History<T, L, true> {
     __device__ __forceinline__ void reset() { next = 0; }
 };
 
+template <class T, int L> struct History<T, L, kHistGlobal> {
+    T* base;       // this lane's element 0
+    int lanes;     // element stride
+    int next;
+    __device__ __forceinline__ void init(void* h) {
+        lanes = int(gridDim.x) * kSliceStride;
+        base = static_cast<T*>(h) + blockIdx.x * kSliceStride + threadIdx.x;
+        next = 0;
+    }
+    __device__ __forceinline__ int stride() const { return lanes; }
+    __device__ __forceinline__ T* row(int j) const {
+        int k = next - 1 - j;
+        k = k < 0 ? k + kHistory : k;
+        return base + size_t(k * 2 * L) * lanes;
+    }
+    __device__ __forceinline__ T s(int j, int l) const { return row(j)[size_t(2 * l) * lanes]; }
+    __device__ __forceinline__ T y(int j, int l) const { return row(j)[size_t(2 * l + 1) * lanes]; }
+    __device__ __forceinline__ void push(const T* sv, const T* yv) {
+        T* p = base + size_t(next * 2 * L) * lanes;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            p[size_t(2 * l) * lanes] = sv[l];
+            p[size_t(2 * l + 1) * lanes] = yv[l];
+        }
+        next = next + 1 == kHistory ? 0 : next + 1;
+    }
+    __device__ __forceinline__ void reset() { next = 0; }
+};
+
 // Per-lane shared-memory slice of the solver: kValues values of T (cold
-// values; with HSMEM the L-BFGS history and the two-loop coefficients), then
+// values; the L-BFGS history when it is kept in shared memory; the two-loop
+// coefficients when the history is not in registers), then
 // kCounters uint32 work counters; element k of a lane at
 // [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
 // A batched launch places one layer-model slot per quad after the slices.
-template <class T, int L, bool HSMEM> struct LaneSlice {
+template <class T, int L, int HS> struct LaneSlice {
     static constexpr int kCold = 3 * L;                                  // best, outer-start point, start-0 seed
-    static constexpr int kCoeff = kCold + 2 * kHistory * L;              // two-loop coefficients (HSMEM)
-    static constexpr int kValues = HSMEM ? kCoeff + 2 * kHistory : kCold;
+    static constexpr int kCoeff = kCold + (HS == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
+    static constexpr int kValues = HS == kHistRegisters ? kCold : kCoeff + 2 * kHistory;
     static constexpr int kCounters = 5;
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
@@ -180,9 +216,9 @@ enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart,
 
 // BATCH: pixels of many images (one layer-count group); the quad's layer
 // models are staged in the shared-memory slot that `m` refers to.
-template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct QuadSolver {
+template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSolver {
     static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
-    using Slice = LaneSlice<T, L, HSMEM>;
+    using Slice = LaneSlice<T, L, HS>;
     const Models<T>* models_;
     const SolverControls& ctl;
     const SolveArgs& a;
@@ -199,7 +235,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     // Method state (this lane's slice).
     T x[L], g[L], d[L], tr[L], ng[L];
     T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
-    History<T, L, HSMEM> hist;
+    History<T, L, HS> hist;
 
     // Per-quad scalars (uniform within the quad).
     int phase, start, outer, it, attempt, bt, valid;
@@ -215,7 +251,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         tol2 = T(ctl.outer_tolerance * ctl.outer_tolerance);
         itol = T(ctl.inner_tolerance);
         phase = kIdle;
-        hist.init();
+        hist.init(a.history);
     }
 
     // The layer models: the kernel parameter, or the quad's shared-memory
@@ -430,7 +466,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
     // per pair, the coefficients kept in the lane's slice (same arithmetic
     // in the same order).
     __device__ __forceinline__ void two_loop(const bool* freev) {
-        if constexpr (HSMEM) two_loop_rolled(freev);
+        if constexpr (HS != kHistRegisters) two_loop_rolled(freev);
         else two_loop_unrolled(freev);
     }
 
@@ -481,6 +517,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
         T scaling = T(1);
         bool have_scaling = false;
         T* coeffs = &Slice::value(Slice::kCoeff);   // coefficient j at [2j], inverse at [2j+1] (times the stride)
+        const int hs = hist.stride();               // element stride of the history
 #pragma unroll 1
         for (int j = 0; j < valid; ++j) {
             const T* h = hist.row(j);
@@ -488,7 +525,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
 #pragma unroll
             for (int l = 0; l < L; ++l)
                 if (freev[l]) {
-                    const T sa = h[2 * l * kSliceStride], yb = h[(2 * l + 1) * kSliceStride];
+                    const T sa = h[size_t(2 * l) * hs], yb = h[size_t(2 * l + 1) * hs];
                     dot += sa * d[l]; sy += sa * yb; ss += sa * sa; yy += yb * yb;
                 }
             Q.sum4(dot, sy, ss, yy);
@@ -497,7 +534,7 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
             const T coeff = dot * inv;
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) d[l] -= coeff * h[(2 * l + 1) * kSliceStride];
+                if (freev[l]) d[l] -= coeff * h[size_t(2 * l + 1) * hs];
             if (!have_scaling && inv > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             coeffs[2 * j * kSliceStride] = coeff;
             coeffs[(2 * j + 1) * kSliceStride] = inv;
@@ -511,12 +548,12 @@ template <class T, int L, bool REFINE, bool HSMEM, bool BATCH = false> struct Qu
             T dot = T(0);
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) dot += h[(2 * l + 1) * kSliceStride] * d[l];
+                if (freev[l]) dot += h[size_t(2 * l + 1) * hs] * d[l];
             dot = Q.sum(dot);
             const T c = coeffs[2 * j * kSliceStride] - dot * coeffs[(2 * j + 1) * kSliceStride];
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) d[l] += c * h[2 * l * kSliceStride];
+                if (freev[l]) d[l] += c * h[size_t(2 * l) * hs];
         }
     }
 

@@ -8,11 +8,17 @@ namespace unb {
 
 // Persistent solve over SolveArgs::n pixels (or SolveArgs::list); the grid
 // is `threads`-wide blocks times the occupancy limit times `sms`.
-// FP32 variants: 0 L-BFGS history in registers; 1, 2, 3, 4 history in shared
-// memory with registers capped for 4, 3, 5, 6 blocks of 128 threads per SM.
-// FP64 variants (history always in shared memory): 0 uncapped registers;
-// 1, 2 capped for 2, 3 blocks per SM.
-constexpr int kFp32Variants = 5, kFp64Variants = 3;
+// FP32 variants: 0 L-BFGS history in registers; 1, 2 history in shared
+// memory with registers capped for 4, 3 blocks of 128 threads per SM; 3, 4
+// history in global memory (SolveArgs::history), registers capped for 5, 6.
+// FP64 variants: 0, 1, 2 history in shared memory with uncapped registers or
+// registers capped for 2, 3 blocks per SM; 3, 4 history in global memory,
+// registers capped for 3, 4 blocks per SM.
+constexpr int kFp32Variants = 5, kFp64Variants = 5;
+inline bool variant_global_history(int variant) { return variant >= 3; }
+// Blocks per SM that a global-history array is sized for (the launch clamps
+// its grid to the array).
+constexpr int kGlobalHistoryBlocksPerSm = 6;
 cudaError_t launch_solve_fp32(int L, bool refine, int variant, const Models<float>& m, const SolverControls& c,
                               const SolveArgs& a, int threads, int sms, cudaStream_t s);
 cudaError_t launch_solve_fp64(int L, bool refine, int variant, const Models<double>& m, const SolverControls& c,

@@ -7,29 +7,29 @@
 namespace unb {
 
 // Dynamic shared memory: every lane's slice (cold values, the L-BFGS
-// history when HSMEM, work counters), then one layer-model slot per quad
+// history when it is kept there, work counters), then one layer-model slot per quad
 // (BATCH).
-template <class T, int L, bool HSMEM, bool BATCH> struct SolveSmem {
-    using Slice = LaneSlice<T, L, HSMEM>;
+template <class T, int L, int HS, bool BATCH> struct SolveSmem {
+    using Slice = LaneSlice<T, L, HS>;
     static size_t bytes(int threads) {
         return Slice::bytes() + (BATCH ? size_t(threads / 4) * sizeof(Models<T>) : 0);
     }
 };
 
 // MINB: blocks per SM the register allocation must allow (launch bounds).
-template <class T, int L, bool REFINE, bool HSMEM, int MINB, bool BATCH>
+template <class T, int L, bool REFINE, int HS, int MINB, bool BATCH>
 __global__ void __launch_bounds__(128, MINB)
 solve_pixels(const __grid_constant__ Models<T> m, const __grid_constant__ SolverControls ctl,
              const __grid_constant__ SolveArgs a) {
-    QuadSolver<T, L, REFINE, HSMEM, BATCH> S(&m, ctl, a);
+    QuadSolver<T, L, REFINE, HS, BATCH> S(&m, ctl, a);
     S.run();
 }
 
-template <class T, int L, bool REFINE, bool HSMEM, int MINB = 1, bool BATCH = false> struct SolveLauncher {
-    using Smem = SolveSmem<T, L, HSMEM, BATCH>;
+template <class T, int L, bool REFINE, int HS, int MINB = 1, bool BATCH = false> struct SolveLauncher {
+    using Smem = SolveSmem<T, L, HS, BATCH>;
 
     static cudaError_t occupancy(int threads, int* blocks_per_sm) {
-        auto k = solve_pixels<T, L, REFINE, HSMEM, MINB, BATCH>;
+        auto k = solve_pixels<T, L, REFINE, HS, MINB, BATCH>;
         const size_t sm = Smem::bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
@@ -40,11 +40,17 @@ template <class T, int L, bool REFINE, bool HSMEM, int MINB = 1, bool BATCH = fa
 
     static cudaError_t launch(const Models<T>& m, const SolverControls& ctl, const SolveArgs& a, int blocks,
                               int threads, cudaStream_t stream) {
-        auto k = solve_pixels<T, L, REFINE, HSMEM, MINB, BATCH>;
+        auto k = solve_pixels<T, L, REFINE, HS, MINB, BATCH>;
         const size_t sm = Smem::bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
             if (e != cudaSuccess) return e;
+        }
+        if constexpr (HS == kHistGlobal) {
+            // Each resident lane owns a slice of the caller's history array.
+            if (!a.history) return cudaErrorInvalidValue;
+            blocks = blocks < a.history_lanes / kSliceStride ? blocks : a.history_lanes / kSliceStride;
+            if (blocks < 1) return cudaErrorInvalidValue;
         }
         k<<<blocks, threads, sm, stream>>>(m, ctl, a);
         return cudaGetLastError();

@@ -16,9 +16,9 @@ namespace unb {
 namespace {
 constexpr int kL = UNB_SOLVER_LAYERS;
 
-template <class T, bool R, bool H, int B, bool BATCH>
+template <class T, bool R, int HS, int B, bool BATCH>
 cudaError_t go(const Models<T>& m, const SolverControls& c, const SolveArgs& a, int threads, int sms, cudaStream_t s) {
-    using Launch = SolveLauncher<T, kL, R, H, B, BATCH>;
+    using Launch = SolveLauncher<T, kL, R, HS, B, BATCH>;
     int per_sm = 0;
     cudaError_t e = Launch::occupancy(threads, &per_sm);
     if (e != cudaSuccess) return e;
@@ -30,11 +30,11 @@ template <bool R, bool BATCH>
 cudaError_t fp32(int variant, const Models<float>& m, const SolverControls& c, const SolveArgs& a, int threads,
                  int sms, cudaStream_t s) {
     switch (variant) {
-    case 0: return go<float, R, false, 1, BATCH>(m, c, a, threads, sms, s);
-    case 1: return go<float, R, true, 4, BATCH>(m, c, a, threads, sms, s);
-    case 2: return go<float, R, true, 3, BATCH>(m, c, a, threads, sms, s);
-    case 3: return go<float, R, true, 5, BATCH>(m, c, a, threads, sms, s);
-    case 4: return go<float, R, true, 6, BATCH>(m, c, a, threads, sms, s);
+    case 0: return go<float, R, kHistRegisters, 1, BATCH>(m, c, a, threads, sms, s);
+    case 1: return go<float, R, kHistShared, 4, BATCH>(m, c, a, threads, sms, s);
+    case 2: return go<float, R, kHistShared, 3, BATCH>(m, c, a, threads, sms, s);
+    case 3: return go<float, R, kHistGlobal, 5, BATCH>(m, c, a, threads, sms, s);
+    case 4: return go<float, R, kHistGlobal, 6, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -43,9 +43,11 @@ template <bool R, bool BATCH>
 cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, const SolveArgs& a, int threads,
                  int sms, cudaStream_t s) {
     switch (variant) {
-    case 0: return go<double, R, true, 1, BATCH>(m, c, a, threads, sms, s);
-    case 1: return go<double, R, true, 2, BATCH>(m, c, a, threads, sms, s);
-    case 2: return go<double, R, true, 3, BATCH>(m, c, a, threads, sms, s);
+    case 0: return go<double, R, kHistShared, 1, BATCH>(m, c, a, threads, sms, s);
+    case 1: return go<double, R, kHistShared, 2, BATCH>(m, c, a, threads, sms, s);
+    case 2: return go<double, R, kHistShared, 3, BATCH>(m, c, a, threads, sms, s);
+    case 3: return go<double, R, kHistGlobal, 3, BATCH>(m, c, a, threads, sms, s);
+    case 4: return go<double, R, kHistGlobal, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

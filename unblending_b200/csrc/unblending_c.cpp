@@ -88,7 +88,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
     std::mutex mutex;
-    Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters;
+    Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters, history;
     Buffer warm, mlp_w, mlp_b;               // warm-start network on the device
     std::vector<float> mlp_uploaded;         // parameters currently in mlp_w / mlp_b
     explicit Context(int dev) : device(dev) {
@@ -232,7 +232,27 @@ int default_fp32_variant(int L, bool refine) {
     return 1;
 }
 
-int fp64_variant(const unblending_solver_options& so) { return so.fp64_variant >= 0 ? so.fp64_variant : 0; }
+// FP64 kernel variant measured on B200 (1024x1024, 5 layers, re-solve of the
+// FP32 misses, first pass / refinement in ms): shared history uncapped 90 / 130,
+// capped for 3 blocks 100 / 159; global history capped for 3 blocks 75.5 / 131,
+// for 4 blocks 75 / 134.
+int default_fp64_variant(bool refine) { return refine ? 0 : 3; }
+int fp64_variant(const unblending_solver_options& so, bool refine) {
+    return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
+}
+
+// Bytes of a global-memory L-BFGS history array for L layers and values of
+// `elem` bytes, sized for kGlobalHistoryBlocksPerSm blocks on every SM.
+size_t history_lanes(int sms) { return size_t(kGlobalHistoryBlocksPerSm) * sms * kSliceStride; }
+size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * 2 * kHistory * L * elem; }
+
+// Points `a` at a history array when the kernel variant keeps its history in
+// global memory.
+void attach_history(SolveArgs& a, void* array, int variant, int sms) {
+    if (!variant_global_history(variant)) return;
+    a.history = array;
+    a.history_lanes = int(history_lanes(sms));
+}
 
 SolverControls controls(const unblending_solver_options& so) {
     SolverControls c;
@@ -377,13 +397,18 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         a.warm = warm;
     }
     const int threads = so.threads_per_block ? so.threads_per_block : 128;
+    // One history array serves the FP32 solve and the FP64 re-solve (they run
+    // one after the other on the stream).
+    void* history = c.history.get<unsigned char>(history_bytes(L, sizeof(double), c.sms));
     if (so.precision == UNBLENDING_PRECISION_FP64) {
-        ck(launch_solve_fp64(L, refine, fp64_variant(so), make_models<double>(layers, L), ctl, a, threads, c.sms, s));
+        attach_history(a, history, fp64_variant(so, refine), c.sms);
+        ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
         ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
     } else {
         const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, refine);
+        attach_history(a, history, variant, c.sms);
         ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
@@ -395,7 +420,9 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
             b.queue = queues + 1;
             b.input_status = nullptr; b.input_failed = nullptr;
             b.warm = nullptr;   // misses fall back to the reference's (cold) start
-            ck(launch_solve_fp64(L, refine, fp64_variant(so), make_models<double>(layers, L), ctl, b, threads, c.sms, s));
+            b.history = nullptr; b.history_lanes = 0;
+            attach_history(b, history, fp64_variant(so, refine), c.sms);
+            ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, b, threads, c.sms, s));
             ++t_launches;
         } else {
             ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -731,6 +758,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 if (so.precision == UNBLENDING_PRECISION_FP64) a.miss_count = G.counts + 1;
                 plan->counts.push_back(G.counts);
                 plan->pixels += total;
+                void* history = plan->alloc<unsigned char>(history_bytes(L, sizeof(double), c.sms));
                 // Autotuner: time each FP32 kernel variant / block size on a
                 // sample of this group's pixels spread over its images.
                 const auto tkey = std::make_pair(L, so.precision);
@@ -743,7 +771,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                         int32_t* d_count = plan->alloc<int32_t>(1);
                         ck(cudaMemcpyAsync(d_sample, sample.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice, s));
                         ck(cudaMemcpyAsync(d_count, &S, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-                        const std::pair<int, int> candidates[3] = {{0, 128}, {2, 128}, {0, 64}};
+                        const std::pair<int, int> candidates[4] = {{1, 128}, {0, 128}, {2, 128}, {1, 64}};
                         float best_ms = 1e30f;
                         std::pair<int, int> best = candidates[0];
                         for (const auto& cand : candidates) {
@@ -751,6 +779,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                             t.jobs = d_table + table.size();   // reference start: the network has not run yet
                             t.list = d_sample; t.list_count = d_count;
                             t.miss_list = nullptr; t.status = nullptr;
+                            attach_history(t, history, cand.first, c.sms);
                             ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
                             ck(cudaEventRecord(c.ev[4], s));
                             ck(launch_solve_batch_fp32(L, cand.first, ctl32, t, cand.second, c.sms, s));
@@ -764,9 +793,12 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     G.variant = c.tuned[tkey].first;
                     G.threads = c.tuned[tkey].second;
                 } else {
-                    G.variant = so.kernel_variant >= 0 ? so.kernel_variant : 0;
+                    G.variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
                     G.threads = so.threads_per_block ? so.threads_per_block : 128;
                 }
+                attach_history(a, history, so.precision == UNBLENDING_PRECISION_FP64 ? fp64_variant(so, false) : G.variant,
+                               c.sms);
+                attach_history(b, history, fp64_variant(so, false), c.sms);
                 gs.push_back(G);
             }
             // Capture every group's work into one graph.
@@ -782,13 +814,13 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                         ++launches;
                     }
                     if (so.precision == UNBLENDING_PRECISION_FP64) {
-                        ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.fp, 128, c.sms, s));
+                        ck(launch_solve_batch_fp64(G.L, fp64_variant(so, false), ctl, G.fp, 128, c.sms, s));
                         ++launches;
                     } else {
                         ck(launch_solve_batch_fp32(G.L, G.variant, ctl32, G.fp, G.threads, c.sms, s));
                         ++launches;
                         if (so.resolve_misses) {
-                            ck(launch_solve_batch_fp64(G.L, fp64_variant(so), ctl, G.re, 128, c.sms, s));
+                            ck(launch_solve_batch_fp64(G.L, fp64_variant(so, false), ctl, G.re, 128, c.sms, s));
                             ++launches;
                         } else {
                             ck(cudaMemcpyAsync(G.counts + 1, G.counts, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -1082,11 +1114,16 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
         a.miss_list = list_a;
         a.miss_count = counts + 0;
         const int threads = so.threads_per_block ? so.threads_per_block : 128;
+        // Kernel variants that keep their history in global memory would need
+        // an array: this entry point runs their shared-memory counterparts
+        // (same results).
+        const int v64 = variant_global_history(fp64_variant(so, false)) ? 0 : fp64_variant(so, false);
         if (so.precision == UNBLENDING_PRECISION_FP64) {
-            ck(launch_solve_fp64(L, false, fp64_variant(so), make_models<double>(layers, L), ctl, a, threads, sms, s));
+            ck(launch_solve_fp64(L, false, v64, make_models<double>(layers, L), ctl, a, threads, sms, s));
             ++t_launches;
         } else {
-            const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
+            int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
+            if (variant_global_history(variant)) variant = 1;
             ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl32, a, threads, sms, s));
             ++t_launches;
             if (so.resolve_misses) {
@@ -1094,7 +1131,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
                 b.list = list_a; b.list_count = counts + 0;
                 b.miss_list = list_b; b.miss_count = counts + 1;
                 b.queue = queues + 1;
-                ck(launch_solve_fp64(L, false, fp64_variant(so), make_models<double>(layers, L), ctl, b, threads, sms, s));
+                ck(launch_solve_fp64(L, false, v64, make_models<double>(layers, L), ctl, b, threads, sms, s));
                 ++t_launches;
             }
         }
