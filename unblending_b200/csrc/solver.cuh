@@ -67,6 +67,12 @@ extern __shared__ __align__(16) unsigned char solver_smem[];
 // lanes, served by L1/L2), which frees shared memory for more resident
 // blocks when the values are wide (FP64).
 enum : int { kHistRegisters = 0, kHistShared = 1, kHistGlobal = 2 };
+// Storage policy of a solve kernel: a history place, optionally with
+// kVectorsShared, which keeps the iterate x, its gradient g and the search
+// direction d (vectors the evaluation does not touch) in the lane's
+// shared-memory slice instead of registers.
+enum : int { kVectorsShared = 4 };
+constexpr int history_of(int storage) { return storage & 3; }
 
 struct Quad {
     unsigned mask;
@@ -112,9 +118,9 @@ struct Quad {
 // slice index 3L + (slot*L + l)*2 + w. Global form: the same ring buffer in
 // SolveArgs::history, element k of lane g at [k * lanes + g] with
 // g = blockIdx.x * kSliceStride + threadIdx.x and lanes = gridDim.x * kSliceStride.
-template <class T, int L, int HS> struct History;
+template <class T, int L, int HS, int BASE> struct History;
 
-template <class T, int L> struct History<T, L, kHistRegisters> {
+template <class T, int L, int BASE> struct History<T, L, kHistRegisters, BASE> {
     T s_[kHistory][L], y_[kHistory][L];
     __device__ __forceinline__ void init(void*) {}
     __device__ __forceinline__ T s(int j, int l) const { return s_[j][l]; }
@@ -130,8 +136,8 @@ template <class T, int L> struct History<T, L, kHistRegisters> {
     __device__ __forceinline__ void reset() {}
 };
 
-template <class T, int L> struct History<T, L, kHistShared> {
-    static constexpr int kBase = 3 * L;   // after the lane slice's cold values
+template <class T, int L, int BASE> struct History<T, L, kHistShared, BASE> {
+    static constexpr int kBase = BASE;    // slice index of the ring buffer
     int next;
     // This lane's pair of age j: element l of s at row(j)[2*l*kSliceStride],
     // of y at row(j)[(2*l + 1)*kSliceStride].
@@ -156,7 +162,7 @@ template <class T, int L> struct History<T, L, kHistShared> {
     __device__ __forceinline__ void reset() { next = 0; }
 };
 
-template <class T, int L> struct History<T, L, kHistGlobal> {
+template <class T, int L, int BASE> struct History<T, L, kHistGlobal, BASE> {
     T* base;       // this lane's element 0
     int lanes;     // element stride
     int next;
@@ -191,10 +197,12 @@ template <class T, int L> struct History<T, L, kHistGlobal> {
 // kCounters uint32 work counters; element k of a lane at
 // [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
 // A batched launch places one layer-model slot per quad after the slices.
-template <class T, int L, int HS> struct LaneSlice {
+template <class T, int L, int S> struct LaneSlice {
     static constexpr int kCold = 3 * L;                                  // best, outer-start point, start-0 seed
-    static constexpr int kCoeff = kCold + (HS == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
-    static constexpr int kValues = HS == kHistRegisters ? kCold : kCoeff + 2 * kHistory;
+    static constexpr int kVec = kCold;                                   // x, g, d (kVectorsShared)
+    static constexpr int kHist = kVec + ((S & kVectorsShared) ? 3 * L : 0);   // history ring (shared history)
+    static constexpr int kCoeff = kHist + (history_of(S) == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
+    static constexpr int kValues = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
     static constexpr int kCounters = 5;
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
@@ -216,9 +224,11 @@ enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart,
 
 // BATCH: pixels of many images (one layer-count group); the quad's layer
 // models are staged in the shared-memory slot that `m` refers to.
-template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSolver {
+template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSolver {
     static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
-    using Slice = LaneSlice<T, L, HS>;
+    using Slice = LaneSlice<T, L, S>;
+    static constexpr int HS = history_of(S);
+    static constexpr bool VS = (S & kVectorsShared) != 0;
     const Models<T>* models_;
     const SolverControls& ctl;
     const SolveArgs& a;
@@ -233,9 +243,10 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
     T ahat[R];           // alpha lane, refinement: filtered alpha targets (pinned alphas)
 
     // Method state (this lane's slice).
-    T x[L], g[L], d[L], tr[L], ng[L];
+    mutable T xr_[VS ? 1 : L], gr_[VS ? 1 : L], dr_[VS ? 1 : L];   // x, g, d in registers (!VS)
+    T tr[L], ng[L];
     T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
-    History<T, L, HS> hist;
+    History<T, L, HS, Slice::kHist> hist;
 
     // Per-quad scalars (uniform within the quad).
     int phase, start, outer, it, attempt, bt, valid;
@@ -263,6 +274,9 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
     }
 
     // ------------------------------------------------------ cold values --
+    __device__ __forceinline__ T& X(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + l); else return xr_[l]; }
+    __device__ __forceinline__ T& G(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + L + l); else return gr_[l]; }
+    __device__ __forceinline__ T& D(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + 2 * L + l); else return dr_[l]; }
     __device__ __forceinline__ T& best(int l) const { return Slice::value(l); }
     __device__ __forceinline__ T& ox(int l) const { return Slice::value(L + l); }
     __device__ __forceinline__ T& init(int l) const { return Slice::value(2 * L + l); }
@@ -303,7 +317,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
     }
     __device__ __forceinline__ bool fixed_at(int l, T gl) const {
         const T lv = lo(l), hv = hi(l);
-        return lv == hv || (x[l] <= lv && gl > T(0)) || (x[l] >= hv && gl < T(0));
+        return lv == hv || (X(l) <= lv && gl > T(0)) || (X(l) >= hv && gl < T(0));
     }
     __device__ __forceinline__ T mean_of(const Models<T>& m, int l) const {
         return colour ? sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
@@ -458,7 +472,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
     // ------------------------------------------------------ bookkeeping --
     __device__ __forceinline__ void steepest() {
 #pragma unroll
-        for (int l = 0; l < L; ++l) d[l] = fixed_at(l, g[l]) ? T(0) : -g[l];
+        for (int l = 0; l < L; ++l) D(l) = fixed_at(l, G(l)) ? T(0) : -G(l);
     }
 
     // Two-loop recursion on the current free set; d holds q on entry/exit.
@@ -482,7 +496,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
                 for (int l = 0; l < L; ++l)
                     if (freev[l]) {
                         const T sa = hist.s(j, l), yb = hist.y(j, l);
-                        dot += sa * d[l]; sy += sa * yb; ss += sa * sa; yy += yb * yb;
+                        dot += sa * D(l); sy += sa * yb; ss += sa * sa; yy += yb * yb;
                     }
                 Q.sum4(dot, sy, ss, yy);
                 const T r = qdiv(T(1), sy);
@@ -490,25 +504,25 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
                 coeff[j] = dot * inv[j];
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) d[l] -= coeff[j] * hist.y(j, l);
+                    if (freev[l]) D(l) -= coeff[j] * hist.y(j, l);
                 if (!have_scaling && inv[j] > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             }
         }
         scaling = fmax(T(1e-12), fmin(T(1e3), scaling));
 #pragma unroll
-        for (int l = 0; l < L; ++l) d[l] *= scaling;
+        for (int l = 0; l < L; ++l) D(l) *= scaling;
 #pragma unroll
         for (int j = kHistory - 1; j >= 0; --j) {
             if (j < valid) {
                 T dot = T(0);
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) dot += hist.y(j, l) * d[l];
+                    if (freev[l]) dot += hist.y(j, l) * D(l);
                 dot = Q.sum(dot);
                 const T c = coeff[j] - dot * inv[j];
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) d[l] += c * hist.s(j, l);
+                    if (freev[l]) D(l) += c * hist.s(j, l);
             }
         }
     }
@@ -526,7 +540,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
             for (int l = 0; l < L; ++l)
                 if (freev[l]) {
                     const T sa = h[size_t(2 * l) * hs], yb = h[size_t(2 * l + 1) * hs];
-                    dot += sa * d[l]; sy += sa * yb; ss += sa * sa; yy += yb * yb;
+                    dot += sa * D(l); sy += sa * yb; ss += sa * sa; yy += yb * yb;
                 }
             Q.sum4(dot, sy, ss, yy);
             const T r = qdiv(T(1), sy);
@@ -534,26 +548,26 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
             const T coeff = dot * inv;
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) d[l] -= coeff * h[size_t(2 * l + 1) * hs];
+                if (freev[l]) D(l) -= coeff * h[size_t(2 * l + 1) * hs];
             if (!have_scaling && inv > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             coeffs[2 * j * kSliceStride] = coeff;
             coeffs[(2 * j + 1) * kSliceStride] = inv;
         }
         scaling = fmax(T(1e-12), fmin(T(1e3), scaling));
 #pragma unroll
-        for (int l = 0; l < L; ++l) d[l] *= scaling;
+        for (int l = 0; l < L; ++l) D(l) *= scaling;
 #pragma unroll 1
         for (int j = valid - 1; j >= 0; --j) {
             const T* h = hist.row(j);
             T dot = T(0);
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) dot += h[size_t(2 * l + 1) * hs] * d[l];
+                if (freev[l]) dot += h[size_t(2 * l + 1) * hs] * D(l);
             dot = Q.sum(dot);
             const T c = coeffs[2 * j * kSliceStride] - dot * coeffs[(2 * j + 1) * kSliceStride];
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) d[l] += c * h[size_t(2 * l) * hs];
+                if (freev[l]) D(l) += c * h[size_t(2 * l) * hs];
         }
     }
 
@@ -573,24 +587,24 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
                 if (!colour) v = REFINE ? init(l) : T(0.5);
                 else v = fmax(T(0.05), fmin(T(0.95), mean_of(m, l)));
             }
-            x[l] = clampb(l, v);
+            X(l) = clampb(l, v);
         }
         if (s == 2) {
             // Move Dodge/Burn sources into the unsaturated branch.
             T av[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) av[l] = Q.from(x[l], 3);
-            T dest = x[0], da = av[0];
+            for (int l = 0; l < L; ++l) av[l] = Q.from(X(l), 3);
+            T dest = X(0), da = av[0];
 #pragma unroll
             for (int l = 1; l < L; ++l) {
                 const T al = av[l];
                 const T Al = T(m.X[l]) * al * da + T(m.Y[l]) * al * (T(1) - da) + T(m.Z[l]) * da * (T(1) - al);
                 if (colour) {
-                    T sv = x[l];
+                    T sv = X(l);
                     if (dest >= T(0) && dest <= T(1) && m.mode[l] == 6) sv = fmin(sv, fmax(T(0), T(1) - dest - T(0.05)));
                     if (dest >= T(0) && dest <= T(1) && m.mode[l] == 7) sv = fmax(sv, fmin(T(1), T(1) - dest + T(0.05)));
                     sv = clampb(l, sv);
-                    x[l] = sv;
+                    X(l) = sv;
                     const T pre = blend_value_call<T>(m.mode[l], sv, dest) * al * da + T(m.Y[l]) * al * (T(1) - da) * sv +
                                   T(m.Z[l]) * da * (T(1) - al) * dest;
                     dest = Al > T(1e-12) ? pre / Al : pre;
@@ -608,7 +622,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
     __device__ __forceinline__ int begin_outer() {
         count(4);
 #pragma unroll
-        for (int l = 0; l < L; ++l) { ox(l) = x[l]; tr[l] = x[l]; }
+        for (int l = 0; l < L; ++l) { ox(l) = X(l); tr[l] = X(l); }
         phase = kOuterEval;
         return aEval;
     }
@@ -631,7 +645,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         if (norm > T(0.0625) * oldnorm) rho *= T(10);
         T motion = T(0);
 #pragma unroll
-        for (int l = 0; l < L; ++l) { const T dl = x[l] - ox(l); motion += dl * dl; }
+        for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion += dl * dl; }
         motion = Q.sum(motion);
         if (!(motion < tol2 && feasible) && outer + 1 < ctl.outer) {
             ++outer;
@@ -652,9 +666,9 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
             T sl = T(0), mo = T(0);
 #pragma unroll
             for (int l = 0; l < L; ++l) {
-                tr[l] = clampb(l, x[l] + step * d[l]);
-                const T delta = tr[l] - x[l];
-                sl += g[l] * delta;
+                tr[l] = clampb(l, X(l) + step * D(l));
+                const T delta = tr[l] - X(l);
+                sl += G(l) * delta;
                 mo += delta * delta;
             }
             Q.sum2(sl, mo);
@@ -674,9 +688,9 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         T pg2 = T(0);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            freev[l] = !fixed_at(l, g[l]);
-            d[l] = freev[l] ? g[l] : T(0);
-            pg2 += d[l] * d[l];
+            freev[l] = !fixed_at(l, G(l));
+            D(l) = freev[l] ? G(l) : T(0);
+            pg2 += D(l) * D(l);
         }
         pg2 = Q.sum(pg2);
         if (pg2 < T(1e-16) || !finite_(f)) return aEndOuter;
@@ -684,11 +698,11 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         T descent = T(0);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            T v = -d[l];
+            T v = -D(l);
             const T lv = lo(l), hv = hi(l);
-            if (lv == hv || (x[l] <= lv && v < T(0)) || (x[l] >= hv && v > T(0))) v = T(0);
-            d[l] = v;
-            descent += v * g[l];
+            if (lv == hv || (X(l) <= lv && v < T(0)) || (X(l) >= hv && v > T(0))) v = T(0);
+            D(l) = v;
+            descent += v * G(l);
         }
         descent = Q.sum(descent);
         if (!(descent < T(0))) { valid = 0; hist.reset(); steepest(); }
@@ -703,10 +717,10 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         T sv[L], yv[L];
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            sv[l] = tr[l] - x[l];
-            yv[l] = ng[l] - g[l];
+            sv[l] = tr[l] - X(l);
+            yv[l] = ng[l] - G(l);
             sy += sv[l] * yv[l]; ss += sv[l] * sv[l]; yy += yv[l] * yv[l];
-            mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(x[l])));
+            mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
         }
         Q.sum3(sy, ss, yy);
         mm = Q.max(mm);
@@ -717,7 +731,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         }
         const T delta = fabs(f - cand), size = T(0.5) * (fabs(f) + fabs(cand));
 #pragma unroll
-        for (int l = 0; l < L; ++l) { x[l] = tr[l]; g[l] = ng[l]; }
+        for (int l = 0; l < L; ++l) { X(l) = tr[l]; G(l) = ng[l]; }
 #pragma unroll
         for (int q = 0; q < R; ++q) resx[q] = res[q];
         f = cand;
@@ -731,7 +745,7 @@ template <class T, int L, bool REFINE, int HS, bool BATCH = false> struct QuadSo
         if (phase == kOuterEval) {
             f = value;
 #pragma unroll
-            for (int l = 0; l < L; ++l) g[l] = ng[l];
+            for (int l = 0; l < L; ++l) G(l) = ng[l];
 #pragma unroll
             for (int q = 0; q < R; ++q) resx[q] = res[q];
             oldnorm = Q.sum(own_norm(res));

@@ -16,9 +16,9 @@ namespace unb {
 namespace {
 constexpr int kL = UNB_SOLVER_LAYERS;
 
-template <class T, bool R, int HS, int B, bool BATCH>
+template <class T, bool R, int S, int B, bool BATCH>
 cudaError_t go(const Models<T>& m, const SolverControls& c, const SolveArgs& a, int threads, int sms, cudaStream_t s) {
-    using Launch = SolveLauncher<T, kL, R, HS, B, BATCH>;
+    using Launch = SolveLauncher<T, kL, R, S, B, BATCH>;
     int per_sm = 0;
     cudaError_t e = Launch::occupancy(threads, &per_sm);
     if (e != cudaSuccess) return e;
@@ -45,9 +45,9 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
     switch (variant) {
     case 0: return go<double, R, kHistShared, 1, BATCH>(m, c, a, threads, sms, s);
     case 1: return go<double, R, kHistShared, 2, BATCH>(m, c, a, threads, sms, s);
-    case 2: return go<double, R, kHistShared, 3, BATCH>(m, c, a, threads, sms, s);
+    case 2: return go<double, R, kHistGlobal | kVectorsShared, 3, BATCH>(m, c, a, threads, sms, s);
     case 3: return go<double, R, kHistGlobal, 3, BATCH>(m, c, a, threads, sms, s);
-    case 4: return go<double, R, kHistGlobal, 4, BATCH>(m, c, a, threads, sms, s);
+    case 4: return go<double, R, kHistGlobal | kVectorsShared, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -232,11 +232,12 @@ int default_fp32_variant(int L, bool refine) {
     return 1;
 }
 
-// FP64 kernel variant measured on B200 (1024x1024, 5 layers, re-solve of the
-// FP32 misses, first pass / refinement in ms): shared history uncapped 90 / 130,
-// capped for 3 blocks 100 / 159; global history capped for 3 blocks 75.5 / 131,
-// for 4 blocks 75 / 134.
-int default_fp64_variant(bool refine) { return refine ? 0 : 3; }
+// FP64 kernel variant measured on B200 (1024x1024, 5 layers; re-solve of the
+// FP32 misses, first pass / refinement, ms): shared history uncapped 91 / 130;
+// global history capped for 3 blocks 76 / 131; global history with x, g, d in
+// shared memory capped for 3 blocks 76 / 122, for 4 blocks 71 / 128. (FP64
+// solve of every pixel: 334 / 321, 320 / 349, 327 / 328, 325 / 365.)
+int default_fp64_variant(bool refine) { return refine ? 2 : 4; }
 int fp64_variant(const unblending_solver_options& so, bool refine) {
     return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
 }
@@ -248,8 +249,8 @@ size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * 
 
 // Points `a` at a history array when the kernel variant keeps its history in
 // global memory.
-void attach_history(SolveArgs& a, void* array, int variant, int sms) {
-    if (!variant_global_history(variant)) return;
+void attach_history(SolveArgs& a, void* array, bool fp64, int variant, int sms) {
+    if (!variant_global_history(fp64, variant)) return;
     a.history = array;
     a.history_lanes = int(history_lanes(sms));
 }
@@ -401,14 +402,14 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     // one after the other on the stream).
     void* history = c.history.get<unsigned char>(history_bytes(L, sizeof(double), c.sms));
     if (so.precision == UNBLENDING_PRECISION_FP64) {
-        attach_history(a, history, fp64_variant(so, refine), c.sms);
+        attach_history(a, history, true, fp64_variant(so, refine), c.sms);
         ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
         ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
     } else {
         const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, refine);
-        attach_history(a, history, variant, c.sms);
+        attach_history(a, history, false, variant, c.sms);
         ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
@@ -421,7 +422,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
             b.input_status = nullptr; b.input_failed = nullptr;
             b.warm = nullptr;   // misses fall back to the reference's (cold) start
             b.history = nullptr; b.history_lanes = 0;
-            attach_history(b, history, fp64_variant(so, refine), c.sms);
+            attach_history(b, history, true, fp64_variant(so, refine), c.sms);
             ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, b, threads, c.sms, s));
             ++t_launches;
         } else {
@@ -779,7 +780,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                             t.jobs = d_table + table.size();   // reference start: the network has not run yet
                             t.list = d_sample; t.list_count = d_count;
                             t.miss_list = nullptr; t.status = nullptr;
-                            attach_history(t, history, cand.first, c.sms);
+                            attach_history(t, history, false, cand.first, c.sms);
                             ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
                             ck(cudaEventRecord(c.ev[4], s));
                             ck(launch_solve_batch_fp32(L, cand.first, ctl32, t, cand.second, c.sms, s));
@@ -796,9 +797,9 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     G.variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
                     G.threads = so.threads_per_block ? so.threads_per_block : 128;
                 }
-                attach_history(a, history, so.precision == UNBLENDING_PRECISION_FP64 ? fp64_variant(so, false) : G.variant,
-                               c.sms);
-                attach_history(b, history, fp64_variant(so, false), c.sms);
+                if (so.precision == UNBLENDING_PRECISION_FP64) attach_history(a, history, true, fp64_variant(so, false), c.sms);
+                else attach_history(a, history, false, G.variant, c.sms);
+                attach_history(b, history, true, fp64_variant(so, false), c.sms);
                 gs.push_back(G);
             }
             // Capture every group's work into one graph.
@@ -1117,13 +1118,13 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
         // Kernel variants that keep their history in global memory would need
         // an array: this entry point runs their shared-memory counterparts
         // (same results).
-        const int v64 = variant_global_history(fp64_variant(so, false)) ? 0 : fp64_variant(so, false);
+        const int v64 = variant_global_history(true, fp64_variant(so, false)) ? 0 : fp64_variant(so, false);
         if (so.precision == UNBLENDING_PRECISION_FP64) {
             ck(launch_solve_fp64(L, false, v64, make_models<double>(layers, L), ctl, a, threads, sms, s));
             ++t_launches;
         } else {
             int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
-            if (variant_global_history(variant)) variant = 1;
+            if (variant_global_history(false, variant)) variant = 1;
             ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl32, a, threads, sms, s));
             ++t_launches;
             if (so.resolve_misses) {
