@@ -18,6 +18,13 @@ reference's refinement radius 60*min(w,h)/1000 = 61.
   e2e        : the plain configuration through the C ABI calls
                unblending_unmix + unblending_refine with pinned host buffers.
 
+Other workloads (`--workload`, extra measurements beside the default line):
+  rgb4096_l6 : the same step on the 4096x4096 six-layer image (soft-light on
+               top, blobs 50-800 px, N(0, 0.01) colour noise, filter r = 8).
+  batch64    : the batched first pass over 64 images (sides 256-2048, 3-6
+               layers, one shared layer set per layer count), plain and with
+               a learned start per layer count.
+
 Multi-GPU: one process per GPU, each decomposing its own image (weak
 scaling, no collective on the data path); time = max over ranks.
 
@@ -53,13 +60,31 @@ SAMPLE = 4096                                        # pixels in the CPU baselin
 SOLVE_TRAFFIC_BYTES_PER_PIXEL = 145.0
 
 
+def load_workload(args, rank=0):
+    """The single-image workload of this run (its own seed + rank)."""
+    from unblending_b200 import synthetic as syn
+    seed = syn.WORKLOADS[args.workload]["seed"] + rank
+    return syn.workload(args.workload, args.width, args.width, seed=seed)
+
+
+def refinement_radius(wl):
+    from unblending_b200 import synthetic as syn
+    return wl.radius if wl.radius is not None else syn.reference_radius(wl.width, wl.height)
+
+
+def workload_label(wl):
+    return (f"{wl.name} {wl.width}x{wl.height} L={len(wl.layers)} unmix+refine(opaque, smooth bg, "
+            f"r={refinement_radius(wl)})")
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--width", type=int, default=1024)
+    p.add_argument("--workload", default=WORKLOAD, choices=["rgb1024_l5", "rgb4096_l6", "batch64"])
+    p.add_argument("--width", type=int, default=None, help="square side (default: the workload's own)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-warm", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
@@ -151,7 +176,7 @@ def cpu_reference(wl, first_gpu, finals, threads, sample_idx):
     rgb_planar = wl.image.reshape(n, 3).T.copy()
     first_x = oracle.unpack(first_gpu, L)
     first_planar = first_x.T.copy()
-    radius = syn.reference_radius(w, h)
+    radius = refinement_radius(wl)
     t0 = time.perf_counter()
     if kind == "reference":
         targets = np.zeros((L + 3, n))
@@ -194,7 +219,9 @@ def reference_arm(args):
     rank, world, _ = dist.env()
     if rank != 0:
         return
-    wl = syn.workload(WORKLOAD, args.width, args.width)
+    if args.workload == "batch64":
+        return reference_batch_arm(args)
+    wl = load_workload(args)
     L, n = len(wl.layers), wl.pixels
     threads = os.cpu_count() or 1
     impl = oracle.ref_lib()
@@ -220,8 +247,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
-        "config": {"workload": f"{WORKLOAD} {args.width}x{args.width} L=5 unmix+refine(opaque, smooth bg, r=ref formula)",
-                   "warm_start": False},
+        "config": {"workload": workload_label(wl), "warm_start": False},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"per step: CPU guided filter over the full image + both solves on {SAMPLE} "
                                    f"seeded pixels, extrapolated to {n} pixels"},
@@ -282,12 +308,14 @@ class Decomposition:
 
 
 def train_warm_start(U, torch, wl):
-    """The warm-start network for this layer set: 64 seeded 256x256 images
-    (2^22 pixels), batch 8192, 512 Adam steps at lr 1e-3."""
+    """The warm-start network for this layer set: 64 seeded 256x256 images of
+    the workload's distributions (2^22 pixels), batch 8192, 512 Adam steps at
+    lr 1e-3."""
     from unblending_b200 import synthetic as syn
     modes = [s.mode for s in wl.layers]
     t0 = time.perf_counter()
-    imgs = [syn.generate(256, 256, modes, (20.0, 200.0), seed=10_000 + k, layers=wl.layers) for k in range(64)]
+    sigma, noise = wl.meta.get("sigma", (20.0, 200.0)), wl.meta.get("noise", 0.0)
+    imgs = [syn.generate(256, 256, modes, sigma, seed=10_000 + k, noise=noise, layers=wl.layers) for k in range(64)]
     d = [torch.from_numpy(w.image.reshape(-1)).cuda() for w in imgs]
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -312,12 +340,13 @@ def b200_arm(args):
     import unblending_b200 as U
     from unblending_b200 import synthetic as syn
 
-    wl = syn.workload(WORKLOAD, args.width, args.width, seed=2 + rank)
+    wl = load_workload(args, rank)
     L, n, w, h = len(wl.layers), wl.pixels, wl.width, wl.height
+    radius = refinement_radius(wl)
     stream = torch.cuda.Stream()
     D = Decomposition(U, torch, wl, stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    plain = U.solver_options(precision=U.PRECISION_FP32)
+    plain = U.solver_options(precision=U.PRECISION_FP32, radius=radius)
 
     sampler = ClockSampler(local)
     if world > 1:
@@ -342,7 +371,7 @@ def b200_arm(args):
     warm = None
     if not args.no_warm:
         model, training = train_warm_start(U, torch, wl)
-        wsolver = U.solver_options(precision=U.PRECISION_FP32, warm_start=model)
+        wsolver = U.solver_options(precision=U.PRECISION_FP32, warm_start=model, radius=radius)
         wms, _ = D.timed(wsolver, args.steps, args.warmup, flush)
         ws1, ws2, _ = D.step(wsolver, counters=True, stats=True)
         torch.cuda.synchronize()
@@ -359,7 +388,7 @@ def b200_arm(args):
     # ---- FP64 solve (replays the reference's FP64 solver)
     fp64 = None
     if not args.no_fp64:
-        fsolver = U.solver_options(precision=U.PRECISION_FP64)
+        fsolver = U.solver_options(precision=U.PRECISION_FP64, radius=radius)
         fms, _ = D.timed(fsolver, max(2, args.steps // 2), 1, flush)
         fp64 = {"value": dist.throughput(n, fms, "cuda"), "ms_per_step": dist.reduce_max(fms, "cuda")}
         first_fp64, final_fp64 = D.host("first"), D.host("final")
@@ -374,11 +403,21 @@ def b200_arm(args):
     dp = ctypes.POINTER(ctypes.c_double)
 
     def e2e_step():
-        rc = U.lib.unblending_unmix(ctypes.byref(view), arr, L, ctypes.byref(opts_unmix),
-                                    host_first.ctypes.data_as(dp), host_first.size)
-        assert rc == 0, rc
-        rc = U.lib.unblending_refine(ctypes.byref(view), arr, L, host_first.ctypes.data_as(dp), host_first.size,
-                                     ctypes.byref(opts_refine), host_out.ctypes.data_as(dp), host_out.size)
+        if wl.radius is None:
+            # The v1 entry points (their radius is the reference's formula).
+            rc = U.lib.unblending_unmix(ctypes.byref(view), arr, L, ctypes.byref(opts_unmix),
+                                        host_first.ctypes.data_as(dp), host_first.size)
+            assert rc == 0, rc
+            rc = U.lib.unblending_refine(ctypes.byref(view), arr, L, host_first.ctypes.data_as(dp), host_first.size,
+                                         ctypes.byref(opts_refine), host_out.ctypes.data_as(dp), host_out.size)
+        else:
+            # The workload names its own radius: the _ex entry points carry it.
+            rc = U.lib.unblending_unmix_ex(ctypes.byref(view), arr, L, ctypes.byref(opts_unmix), ctypes.byref(plain),
+                                           host_first.ctypes.data_as(dp), host_first.size, None, None, None)
+            assert rc == 0, rc
+            rc = U.lib.unblending_refine_ex(ctypes.byref(view), arr, L, host_first.ctypes.data_as(dp),
+                                            host_first.size, ctypes.byref(opts_refine), ctypes.byref(plain),
+                                            host_out.ctypes.data_as(dp), host_out.size, None, None, None)
         assert rc == 0, rc
 
     for _ in range(max(1, args.warmup - 1)):
@@ -410,7 +449,7 @@ def b200_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
-        "config": {"workload": f"{WORKLOAD} {w}x{h} L=5 unmix+refine(opaque, smooth bg, r={s2['radius']})",
+        "config": {"workload": workload_label(wl),
                    "precision": "fp32 solve + fp64 check/re-solve of misses", "warm_start": False, "starts": 1,
                    "l2": "256 MiB buffer written between steps, outside the timed region",
                    "parallelism": f"{world} independent images (one per GPU)"},
@@ -455,10 +494,142 @@ def b200_arm(args):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------------------- batch64 --
+BATCH_COUNT = 64
+
+
+def batch_workload(rank=0):
+    from unblending_b200 import synthetic as syn
+    return syn.batch(count=BATCH_COUNT, seed=4 + rank, sides=(256, 2048), shared_layers=True)
+
+
+def batch_label(wls):
+    Ls = sorted({len(w.layers) for w in wls})
+    return (f"batch64: {len(wls)} images, sides 256-2048, layers {Ls[0]}-{Ls[-1]} (one layer set per count), "
+            f"{sum(w.pixels for w in wls)} pixels, first pass")
+
+
+def batch_arm(args):
+    """The batched first pass (one persistent launch per layer count, one
+    captured graph), plain and with a learned start per layer count."""
+    import torch
+    from unblending_b200 import dist
+    rank, world, local = dist.env()
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    import unblending_b200 as U
+    wls = batch_workload(rank)
+    n = sum(w.pixels for w in wls)
+    imgs = [torch.from_numpy(w.image.reshape(-1)).cuda() for w in wls]
+    outs = [torch.empty(4 * len(w.layers) * w.pixels, dtype=torch.float64, device="cuda") for w in wls]
+    sts = [torch.empty(w.pixels, dtype=torch.int32, device="cuda") for w in wls]
+    stream = torch.cuda.Stream()
+    ext = torch.cuda.ExternalStream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def jobs(nets):
+        return [dict(width=w.width, height=w.height, d_image=i.data_ptr(), layers=w.layers, d_output=o.data_ptr(),
+                     d_status=s.data_ptr(), warm_start=nets.get(len(w.layers)) if nets else None)
+                for w, i, o, s in zip(wls, imgs, outs, sts)]
+
+    def timed(job_list):
+        st = U.unmix_batch_device(job_list, stream=stream.cuda_stream, stats=True)   # plan, autotune, graph
+        for _ in range(max(0, args.warmup - 1)):
+            U.unmix_batch_device(job_list, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            U.unmix_batch_device(job_list, stream=stream.cuda_stream)
+            e1.record(ext)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return float(np.mean(times)), st, U.last_launch_count()
+
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    sampler.start()
+    ms, st, launches = timed(jobs(None))
+    clocks = sampler.stop()
+    nets, training = {}, {}
+    for L in sorted({len(w.layers) for w in wls}):
+        ref = next(w for w in wls if len(w.layers) == L)
+        nets[L], training[L] = train_warm_start(U, torch, ref)
+    wms, wst, _ = timed(jobs(nets))
+    line = {
+        "metric": "pixels/sec, batched first pass, warm-start vs plain", "value": dist.throughput(n, ms, "cuda"),
+        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dist.reduce_max(ms, "cuda"), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, unblending_b200/synthetic.py)",
+        "config": {"workload": batch_label(wls), "precision": "fp32 solve + fp64 check/re-solve of misses",
+                   "l2": "256 MiB buffer written between steps, outside the timed region"},
+        "clocks": clocks, "gpu_launches": launches * args.steps,
+        "plain": {"misses": st["misses"], "failed": st["failed"]},
+        "warm_start": {"value": dist.throughput(n, wms, "cuda"), "ms_per_step": dist.reduce_max(wms, "cuda"),
+                       "speedup_vs_plain": ms / wms, "misses": wst["misses"], "failed": wst["failed"],
+                       "training_final_batch_mse": {L: t["final_batch_mse"] for L, t in training.items()}},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def reference_batch_arm(args):
+    """The reference's FP64 solver on a 4096-pixel sample spread over the
+    batch's images (first pass), extrapolated to all of its pixels."""
+    import oracle
+    from unblending_b200 import synthetic as syn
+    wls = batch_workload()
+    n = sum(w.pixels for w in wls)
+    threads = os.cpu_count() or 1
+    impl = oracle.ref_lib()
+    kind = "reference" if impl is not None else "port"
+    impl = impl or oracle.lib()
+    rng = np.random.default_rng(0)
+    per = [max(1, int(round(SAMPLE * w.pixels / n))) for w in wls]
+    samples = [np.sort(rng.choice(w.pixels, size=min(k, w.pixels), replace=False)) for w, k in zip(wls, per)]
+    times = []
+    for step in range(args.warmup + args.steps):
+        t, m = 0.0, 0
+        for w, idx in zip(wls, samples):
+            L = len(w.layers)
+            t0 = time.perf_counter()
+            impl.solve(syn.layer_array(w.layers), oracle.problem(L, False, True), oracle.options(),
+                       w.image.reshape(-1, 3)[idx], np.tile(oracle.initial_first(w.layers, True), (len(idx), 1)),
+                       threads=threads)
+            t += (time.perf_counter() - t0) * w.pixels / len(idx)
+        if step >= args.warmup:
+            times.append(t)
+    sec = float(np.mean(times))
+    value = n / sec
+    line = {
+        "impl": "reference", "metric": "pixels/sec, batched first pass, warm-start vs plain", "value": value,
+        "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, unblending_b200/synthetic.py)", "config": {"workload": batch_label(wls)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"per step: first-pass solves of {sum(len(x) for x in samples)} seeded pixels "
+                                   f"spread over the images, extrapolated to {n} pixels"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "batch64":
+        batch_arm(args)
     else:
         b200_arm(args)
 

@@ -232,13 +232,21 @@ BATCH_MODES = [M["normal"], M["multiply"], M["screen"], M["overlay"], M["color_d
 
 
 def batch(count: int = 64, seed: int = 4, sides: tuple[int, int] = (256, 2048),
-          layers: tuple[int, int] = (3, 6)) -> list[Workload]:
+          layers: tuple[int, int] = (3, 6), shared_layers: bool = False) -> list[Workload]:
     """Images of uneven size and layer count: side ~ U{sides}, aspect 1:1 to
     4:3 (either orientation), L ~ U{layers}, modes drawn from normal,
     multiply, screen, overlay, color-dodge, soft-light, color-burn (bottom
-    layer normal), blobs 20-200 px, each image with its own seed."""
+    layer normal), blobs 20-200 px, each image with its own seed. With
+    `shared_layers`, all images of one layer count share one layer set (modes
+    and colour models), as the images a learned start is trained for do."""
     rng = np.random.default_rng(seed)
     out = []
+    sets = {}
+    if shared_layers:
+        srng = np.random.default_rng([seed, 104729])
+        for L in range(layers[0], layers[1] + 1):
+            modes = [M["normal"]] + [int(m) for m in srng.choice(BATCH_MODES, size=L - 1)]
+            sets[L] = make_layers(srng, modes)
     for k in range(count):
         side = int(rng.integers(sides[0], sides[1] + 1))
         aspect = rng.uniform(1.0, 4.0 / 3.0)
@@ -247,7 +255,11 @@ def batch(count: int = 64, seed: int = 4, sides: tuple[int, int] = (256, 2048),
             w, h = h, w
         L = int(rng.integers(layers[0], layers[1] + 1))
         modes = [M["normal"]] + [int(m) for m in rng.choice(BATCH_MODES, size=L - 1)]
-        out.append(generate(w, h, modes, (20.0, 200.0), seed=int(rng.integers(1 << 31)), name=f"batch{k}"))
+        shared = sets.get(L)
+        if shared is not None:
+            modes = [spec.mode for spec in shared]
+        out.append(generate(w, h, modes, (20.0, 200.0), seed=int(rng.integers(1 << 31)), name=f"batch{k}",
+                            layers=shared))
     return out
 
 
