@@ -153,7 +153,9 @@ UNBLENDING_API int32_t unblending_refine_device(
  * buffers (device memory). The solve's scratch (queue heads, miss counters,
  * miss lists) lives in a fixed 32 MiB + 256 B device array that every GPU
  * loading the library holds until the process exits; images larger than
- * 2048 * 2048 = 4,194,304 pixels return UNBLENDING_INVALID_ARGUMENT. The call
+ * 2048 * 2048 = 4,194,304 pixels return UNBLENDING_INVALID_ARGUMENT. Kernel
+ * variants that keep their L-BFGS history in global memory are replaced by
+ * their shared-memory counterparts (same results). The call
  * uses no cudaMalloc, cudaFree, library stream or event; work is enqueued on
  * `stream` (NULL: the legacy default stream) and the call returns without
  * synchronizing. The first call on a device resolves the array's device
