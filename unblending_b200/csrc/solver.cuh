@@ -431,7 +431,30 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 const T db = X * av - Y * av + Z * (T(1) - av);
                 const bool big = Al > T(1e-12);
                 T ga, gp;
-                if (colour) {
+                if constexpr (kFast) {
+                    // FP32: the colour channel terms on all four lanes without
+                    // a branch (lane 3 would idle through them anyway; its
+                    // values are replaced by the alpha chain's terms below).
+                    const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
+                    T fv, fs, fd;
+                    blend3(m, l, s, c, fv, fs, fd);
+                    const T ds = av * dd * fs + Y * av * (T(1) - dd);
+                    const T dc = av * dd * fd + Z * dd * (T(1) - av);
+                    const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
+                    const T pd = fv * av - Y * av * s + Z * (T(1) - av) * c;
+                    const T r = big ? qdiv(T(1), Al) : T(1);
+                    T gs, ad;
+                    if (big) {
+                        ga = v * ((pa - out * da) * r);
+                        gp = v * ((pd - out * db) * r);
+                        gs = v * (ds * r);
+                        ad = v * (dc * r);
+                    } else {
+                        ga = v * pa; gp = v * pd; gs = v * ds; ad = v * dc;
+                    }
+                    if (colour) { ng[l] += gs; adj = ad; }
+                    else { ga = adj3 * da; gp = adj3 * db; }
+                } else if (colour) {
                     const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);
@@ -440,18 +463,10 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
                     const T pd = fv * av - Y * av * s + Z * (T(1) - av) * c;
                     if (big) {
-                        if constexpr (kFast) {
-                            const T r = qdiv(T(1), Al);
-                            ga = v * ((pa - out * da) * r);
-                            gp = v * ((pd - out * db) * r);
-                            ng[l] += v * (ds * r);
-                            adj = v * (dc * r);
-                        } else {
-                            ga = v * ((pa - out * da) / Al);
-                            gp = v * ((pd - out * db) / Al);
-                            ng[l] += v * (ds / Al);
-                            adj = v * (dc / Al);
-                        }
+                        ga = v * ((pa - out * da) / Al);
+                        gp = v * ((pd - out * db) / Al);
+                        ng[l] += v * (ds / Al);
+                        adj = v * (dc / Al);
                     } else {
                         ga = v * pa; gp = v * pd;
                         ng[l] += v * ds;
