@@ -131,8 +131,8 @@ __device__ __forceinline__ void blend_table(const M& m, int l, T s, T d, T& f, T
         const T cs = c ? m.cs[l][0] : m.cs[l][1];
         const T cd = c ? m.cd[l][0] : m.cd[l][1];
         const T csd = c ? m.csd[l][0] : m.csd[l][1];
-        f = c0 + cs * s + cd * d + csd * s * d;
-        if (partials) { fs = cs + csd * d; fd = cd + csd * s; }
+        f = __fmaf_rn(csd * s, d, __fmaf_rn(cd, d, __fmaf_rn(cs, s, c0)));
+        if (partials) { fs = __fmaf_rn(csd, d, cs); fd = __fmaf_rn(csd, s, cd); }
         return;
     }
     blend_special<T>(sp, s, d, f, fs, fd, partials);

@@ -52,6 +52,17 @@ template <class T> __device__ __forceinline__ bool finite_(T v);
 template <> __device__ __forceinline__ bool finite_<float>(float v) { return isfinite(v); }
 template <> __device__ __forceinline__ bool finite_<double>(double v) { return isfinite(v); }
 
+// a*b + c: one fused operation in the FP32 solver (shorter dependency chains,
+// fewer instructions; the same in every kernel variant); a rounded multiply
+// then a rounded add in FP64, as the reference computes it. Every FP64
+// expression written with madd below keeps the reference's operation order
+// (addition commutes exactly in IEEE arithmetic).
+template <class T> __device__ __forceinline__ T madd(T a, T b, T c);
+template <> __device__ __forceinline__ float madd<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <> __device__ __forceinline__ double madd<double>(double a, double b, double c) {
+    return __dadd_rn(__dmul_rn(a, b), c);
+}
+
 // The FP64 blend functions (a switch over the thirteen modes) out of line:
 // one copy of each serves every unrolled layer, which keeps the solver's loop
 // small for the instruction cache. The FP32 solver uses blend_table.
@@ -355,11 +366,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 #pragma unroll
         for (int l = 1; l < L; ++l) {
             const T av = al[l], dd = A[l - 1];
-            const T Al = T(m.X[l]) * av * dd + T(m.Y[l]) * av * (T(1) - dd) + T(m.Z[l]) * dd * (T(1) - av);
+            // X a d + Y a (1 - d) + Z d (1 - a), and the colour the same way.
+            const T Al = madd(T(m.Z[l]) * dd, T(1) - av, madd(T(m.X[l]) * av, dd, T(m.Y[l]) * av * (T(1) - dd)));
             A[l] = Al;
             const T s = tr[l], c = pc[l - 1];
-            const T pre = blend(m, l, s, c) * av * dd + T(m.Y[l]) * av * (T(1) - dd) * s +
-                          T(m.Z[l]) * dd * (T(1) - av) * c;
+            const T pre = madd(T(m.Z[l]) * dd * (T(1) - av), c,
+                               madd(blend(m, l, s, c) * av, dd, T(m.Y[l]) * av * (T(1) - dd) * s));
             pc[l] = Al > T(1e-12) ? qdiv(pre, Al) : pre;
         }
         T energy = T(0), asum = T(0);
@@ -368,17 +380,17 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T mine = colour ? tr[l] - mean_of(m, l) : T(0);
             const T d0 = Q.from(mine, 0), d1 = Q.from(mine, 1), d2 = Q.from(mine, 2);
             const T* P = m.prec[l];
-            const T v0 = P[0] * d0 + P[1] * d1 + P[2] * d2;
-            const T v1 = P[3] * d0 + P[4] * d1 + P[5] * d2;
-            const T v2 = P[6] * d0 + P[7] * d1 + P[8] * d2;
-            const T D = d0 * v0 + d1 * v1 + d2 * v2;
+            const T v0 = madd(P[2], d2, madd(P[0], d0, P[1] * d1));
+            const T v1 = madd(P[5], d2, madd(P[3], d0, P[4] * d1));
+            const T v2 = madd(P[8], d2, madd(P[6], d0, P[7] * d1));
+            const T D = madd(d2, v2, madd(d0, v0, d1 * v1));
             energy += al[l] * D;
             asum += al[l];
             if (need_grad) {
                 if (colour) {
                     const T vq = sel3(Q.q, v0, v1, v2);
-                    const T tq = sel3(Q.q, P[0], P[1], P[2]) * d0 + sel3(Q.q, P[3], P[4], P[5]) * d1 +
-                                 sel3(Q.q, P[6], P[7], P[8]) * d2;
+                    const T tq = madd(sel3(Q.q, P[6], P[7], P[8]), d2,
+                                      madd(sel3(Q.q, P[0], P[1], P[2]), d0, sel3(Q.q, P[3], P[4], P[5]) * d1));
                     ng[l] = al[l] * (vq + tq);
                 } else {
                     ng[l] = D + (REFINE ? T(0) : T(0.01));
@@ -427,8 +439,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             for (int l = L - 1; l > 0; --l) {
                 const T av = al[l], dd = A[l - 1], Al = A[l];
                 const T X = T(m.X[l]), Y = T(m.Y[l]), Z = T(m.Z[l]);
-                const T da = X * dd + Y * (T(1) - dd) - Z * dd;
-                const T db = X * av - Y * av + Z * (T(1) - av);
+                const T da = madd(X, dd, Y * (T(1) - dd)) - Z * dd;
+                const T db = madd(Z, T(1) - av, X * av - Y * av);
                 const bool big = Al > T(1e-12);
                 T ga, gp;
                 if constexpr (kFast) {
@@ -438,15 +450,15 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);
-                    const T ds = av * dd * fs + Y * av * (T(1) - dd);
-                    const T dc = av * dd * fd + Z * dd * (T(1) - av);
-                    const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
-                    const T pd = fv * av - Y * av * s + Z * (T(1) - av) * c;
+                    const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
+                    const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
+                    const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
+                    const T pd = madd(Z * (T(1) - av), c, fv * av - Y * av * s);
                     const T r = big ? qdiv(T(1), Al) : T(1);
                     T gs, ad;
                     if (big) {
-                        ga = v * ((pa - out * da) * r);
-                        gp = v * ((pd - out * db) * r);
+                        ga = v * (madd(-out, da, pa) * r);
+                        gp = v * (madd(-out, db, pd) * r);
                         gs = v * (ds * r);
                         ad = v * (dc * r);
                     } else {
@@ -458,10 +470,10 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);
-                    const T ds = av * dd * fs + Y * av * (T(1) - dd);
-                    const T dc = av * dd * fd + Z * dd * (T(1) - av);
-                    const T pa = fv * dd + Y * (T(1) - dd) * s - Z * dd * c;
-                    const T pd = fv * av - Y * av * s + Z * (T(1) - av) * c;
+                    const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
+                    const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
+                    const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
+                    const T pd = madd(Z * (T(1) - av), c, fv * av - Y * av * s);
                     if (big) {
                         ga = v * ((pa - out * da) / Al);
                         gp = v * ((pd - out * db) / Al);
