@@ -384,7 +384,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T v1 = madd(P[5], d2, madd(P[3], d0, P[4] * d1));
             const T v2 = madd(P[8], d2, madd(P[6], d0, P[7] * d1));
             const T D = madd(d2, v2, madd(d0, v0, d1 * v1));
-            energy += al[l] * D;
+            energy = madd(al[l], D, energy);
             asum += al[l];
             if (need_grad) {
                 if (colour) {
@@ -401,18 +401,18 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         T terms = T(0), norm = T(0);
         if (colour) {
             res[0] = pc[L - 1] - target;
-            terms = T(0.5) * rho * res[0] * res[0] - lam[0] * res[0];
+            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
             norm = res[0] * res[0];
         } else if (REFINE) {
 #pragma unroll
             for (int l = 0; l < R; ++l) {
                 res[l] = tr[l] - ahat[l];
-                terms += T(0.5) * rho * res[l] * res[l] - lam[l] * res[l];
-                norm += res[l] * res[l];
+                terms += madd(T(0.5) * rho * res[l], res[l], -(lam[l] * res[l]));
+                norm = madd(res[l], res[l], norm);
             }
         } else {
             res[0] = A[L - 1] - T(1);
-            terms = T(0.5) * rho * res[0] * res[0] - lam[0] * res[0];
+            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
             norm = res[0] * res[0];
         }
         Q.sum2(terms, norm);
@@ -523,7 +523,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 for (int l = 0; l < L; ++l)
                     if (freev[l]) {
                         const T sa = hist.s(j, l), yb = hist.y(j, l);
-                        dot += sa * D(l); sy += sa * yb; ss += sa * sa; yy += yb * yb;
+                        dot = madd(sa, D(l), dot); sy = madd(sa, yb, sy); ss = madd(sa, sa, ss); yy = madd(yb, yb, yy);
                     }
                 Q.sum4(dot, sy, ss, yy);
                 const T r = qdiv(T(1), sy);
@@ -531,7 +531,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 coeff[j] = dot * inv[j];
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) D(l) -= coeff[j] * hist.y(j, l);
+                    if (freev[l]) D(l) = madd(-coeff[j], hist.y(j, l), D(l));
                 if (!have_scaling && inv[j] > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             }
         }
@@ -544,12 +544,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 T dot = T(0);
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) dot += hist.y(j, l) * D(l);
+                    if (freev[l]) dot = madd(hist.y(j, l), D(l), dot);
                 dot = Q.sum(dot);
-                const T c = coeff[j] - dot * inv[j];
+                const T c = madd(-dot, inv[j], coeff[j]);
 #pragma unroll
                 for (int l = 0; l < L; ++l)
-                    if (freev[l]) D(l) += c * hist.s(j, l);
+                    if (freev[l]) D(l) = madd(c, hist.s(j, l), D(l));
             }
         }
     }
@@ -567,7 +567,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             for (int l = 0; l < L; ++l)
                 if (freev[l]) {
                     const T sa = h[size_t(2 * l) * hs], yb = h[size_t(2 * l + 1) * hs];
-                    dot += sa * D(l); sy += sa * yb; ss += sa * sa; yy += yb * yb;
+                    dot = madd(sa, D(l), dot); sy = madd(sa, yb, sy); ss = madd(sa, sa, ss); yy = madd(yb, yb, yy);
                 }
             Q.sum4(dot, sy, ss, yy);
             const T r = qdiv(T(1), sy);
@@ -575,7 +575,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T coeff = dot * inv;
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) D(l) -= coeff * h[size_t(2 * l + 1) * hs];
+                if (freev[l]) D(l) = madd(-coeff, h[size_t(2 * l + 1) * hs], D(l));
             if (!have_scaling && inv > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             coeffs[2 * j * kSliceStride] = coeff;
             coeffs[(2 * j + 1) * kSliceStride] = inv;
@@ -589,12 +589,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             T dot = T(0);
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) dot += h[size_t(2 * l + 1) * hs] * D(l);
+                if (freev[l]) dot = madd(h[size_t(2 * l + 1) * hs], D(l), dot);
             dot = Q.sum(dot);
-            const T c = coeffs[2 * j * kSliceStride] - dot * coeffs[(2 * j + 1) * kSliceStride];
+            const T c = madd(-dot, coeffs[(2 * j + 1) * kSliceStride], coeffs[2 * j * kSliceStride]);
 #pragma unroll
             for (int l = 0; l < L; ++l)
-                if (freev[l]) D(l) += c * h[size_t(2 * l) * hs];
+                if (freev[l]) D(l) = madd(c, h[size_t(2 * l) * hs], D(l));
         }
     }
 
@@ -668,11 +668,11 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const T norm = Q.sum(own_norm(resx));
         const bool feasible = norm < tol2;
 #pragma unroll
-        for (int r = 0; r < R; ++r) lam[r] -= rho * resx[r];
+        for (int r = 0; r < R; ++r) lam[r] = madd(-rho, resx[r], lam[r]);
         if (norm > T(0.0625) * oldnorm) rho *= T(10);
         T motion = T(0);
 #pragma unroll
-        for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion += dl * dl; }
+        for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion = madd(dl, dl, motion); }
         motion = Q.sum(motion);
         if (!(motion < tol2 && feasible) && outer + 1 < ctl.outer) {
             ++outer;
@@ -693,10 +693,10 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             T sl = T(0), mo = T(0);
 #pragma unroll
             for (int l = 0; l < L; ++l) {
-                tr[l] = clampb(l, X(l) + step * D(l));
+                tr[l] = clampb(l, madd(step, D(l), X(l)));
                 const T delta = tr[l] - X(l);
-                sl += G(l) * delta;
-                mo += delta * delta;
+                sl = madd(G(l), delta, sl);
+                mo = madd(delta, delta, mo);
             }
             Q.sum2(sl, mo);
             if (mo != T(0)) { slope = sl; phase = kTrial; return aEval; }
@@ -717,7 +717,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         for (int l = 0; l < L; ++l) {
             freev[l] = !fixed_at(l, G(l));
             D(l) = freev[l] ? G(l) : T(0);
-            pg2 += D(l) * D(l);
+            pg2 = madd(D(l), D(l), pg2);
         }
         pg2 = Q.sum(pg2);
         if (pg2 < T(1e-16) || !finite_(f)) return aEndOuter;
@@ -729,7 +729,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T lv = lo(l), hv = hi(l);
             if (lv == hv || (X(l) <= lv && v < T(0)) || (X(l) >= hv && v > T(0))) v = T(0);
             D(l) = v;
-            descent += v * G(l);
+            descent = madd(v, G(l), descent);
         }
         descent = Q.sum(descent);
         if (!(descent < T(0))) { valid = 0; hist.reset(); steepest(); }
@@ -746,7 +746,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         for (int l = 0; l < L; ++l) {
             sv[l] = tr[l] - X(l);
             yv[l] = ng[l] - G(l);
-            sy += sv[l] * yv[l]; ss += sv[l] * sv[l]; yy += yv[l] * yv[l];
+            sy = madd(sv[l], yv[l], sy); ss = madd(sv[l], sv[l], ss); yy = madd(yv[l], yv[l], yy);
             mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
         }
         Q.sum3(sy, ss, yy);
