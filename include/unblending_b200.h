@@ -41,7 +41,10 @@ typedef struct unblending_solver_options {
     int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1/2 in shared memory
                                    with registers capped for 4/3 blocks per SM, 3/4 in global memory capped
                                    for 5/6 blocks per SM */
-    const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start */
+    const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start.
+                                   With FP32 precision and resolve_misses, pixels the learned start leaves
+                                   unsolved get the plain FP32 solve from the reference's start, and what
+                                   that misses the FP64 re-solve (the plain path's fallback). */
     int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default; history in shared memory with 0
                                    uncapped registers, 1/2 capped for 2/3 blocks per SM; history in global
                                    memory with 3/4 capped for 3/4 blocks per SM */

@@ -414,13 +414,34 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
         if (so.resolve_misses) {
+            // Misses of a learned start first fall back to the plain FP32
+            // solve from the reference's start (queue 2, its misses counted in
+            // slot 3 of the queue words); what that misses, and the plain
+            // solve's own misses, get the FP64 re-solve from the reference's
+            // start.
+            int32_t* list_a = a.miss_list;
+            int32_t* list_b = c.list_b.get<int32_t>(n);
+            int32_t* fp64_list = list_a;
+            int32_t* fp64_count = counts + 0;
+            int32_t* fp64_misses = list_b;
+            if (a.warm) {
+                SolveArgs w = a;
+                w.list = list_a; w.list_count = counts + 0;
+                w.miss_list = list_b; w.miss_count = reinterpret_cast<int32_t*>(queues + 3);
+                w.queue = queues + 2;
+                w.input_status = nullptr; w.input_failed = nullptr;
+                w.warm = nullptr;
+                ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, w, threads, c.sms, s));
+                ++t_launches;
+                fp64_list = list_b; fp64_count = w.miss_count; fp64_misses = list_a;
+            }
             SolveArgs b = a;
-            b.list = a.miss_list; b.list_count = counts + 0;
-            b.miss_list = c.list_b.get<int32_t>(n);
+            b.list = fp64_list; b.list_count = fp64_count;
+            b.miss_list = fp64_misses;
             b.miss_count = counts + 1;
             b.queue = queues + 1;
             b.input_status = nullptr; b.input_failed = nullptr;
-            b.warm = nullptr;   // misses fall back to the reference's (cold) start
+            b.warm = nullptr;   // the reference's (cold) start
             b.history = nullptr; b.history_lanes = 0;
             attach_history(b, history, true, fp64_variant(so, refine), c.sms);
             ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, b, threads, c.sms, s));
@@ -681,7 +702,8 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
             const SolverControls ctl = controls(so), ctl32 = fp32_controls(so);
             struct Group {
                 int L;
-                SolveArgs fp, re;      // first solve (warm where given), FP64 re-solve (reference start)
+                SolveArgs fp, mid, re;   // first solve (warm where given), FP32 re-solve of its misses from
+                                         // the reference start (groups with a learned start), FP64 re-solve
                 uint32_t* queues;
                 int32_t* counts;
                 std::vector<std::pair<int, float*>> infer;   // job, warm slice
@@ -755,6 +777,20 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 b.list = lists; b.list_count = G.counts + 0;
                 b.miss_list = lists + total; b.miss_count = G.counts + 1;
                 b.queue = G.queues + 1;
+                if (!G.infer.empty()) {
+                    // As the single-image pass: the learned start's misses get the
+                    // plain FP32 solve first (cold jobs of the group repeat theirs,
+                    // with the same result), its misses the FP64 re-solve.
+                    SolveArgs& w = G.mid;
+                    w = a;
+                    w.jobs = d_table + table.size();
+                    w.models = d_m32;
+                    w.list = lists; w.list_count = G.counts + 0;
+                    w.miss_list = lists + total; w.miss_count = reinterpret_cast<int32_t*>(G.queues + 3);
+                    w.queue = G.queues + 2;
+                    b.list = lists + total; b.list_count = w.miss_count;
+                    b.miss_list = lists;
+                }
                 a.models = so.precision == UNBLENDING_PRECISION_FP64 ? static_cast<const void*>(d_m64) : d_m32;
                 if (so.precision == UNBLENDING_PRECISION_FP64) a.miss_count = G.counts + 1;
                 plan->counts.push_back(G.counts);
@@ -799,6 +835,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 }
                 if (so.precision == UNBLENDING_PRECISION_FP64) attach_history(a, history, true, fp64_variant(so, false), c.sms);
                 else attach_history(a, history, false, G.variant, c.sms);
+                attach_history(G.mid, history, false, G.variant, c.sms);
                 attach_history(b, history, true, fp64_variant(so, false), c.sms);
                 gs.push_back(G);
             }
@@ -820,6 +857,10 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     } else {
                         ck(launch_solve_batch_fp32(G.L, G.variant, ctl32, G.fp, G.threads, c.sms, s));
                         ++launches;
+                        if (so.resolve_misses && !G.infer.empty()) {
+                            ck(launch_solve_batch_fp32(G.L, G.variant, ctl32, G.mid, G.threads, c.sms, s));
+                            ++launches;
+                        }
                         if (so.resolve_misses) {
                             ck(launch_solve_batch_fp64(G.L, fp64_variant(so, false), ctl, G.re, 128, c.sms, s));
                             ++launches;
