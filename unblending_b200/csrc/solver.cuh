@@ -19,7 +19,7 @@
 // values of every vector. The five vectors the inner loop touches on every
 // step (x, gradient, direction, trial point, trial gradient) live in
 // registers; the cold ones (best point, the outer step's start point, the
-// start-0 seed) and the work counters live in a per-lane shared-memory slice,
+// start-0 seed) live in a per-lane shared-memory slice,
 // and so does the L-BFGS history in the shared-history variants (the
 // register variant keeps it as a shift register). The composite is separable
 // per channel given the alphas, which lane 3 broadcasts; the 3x3 colour prior
@@ -204,9 +204,8 @@ template <class T, int L, int BASE> struct History<T, L, kHistGlobal, BASE> {
 
 // Per-lane shared-memory slice of the solver: kValues values of T (cold
 // values; the L-BFGS history when it is kept in shared memory; the two-loop
-// coefficients when the history is not in registers), then
-// kCounters uint32 work counters; element k of a lane at
-// [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
+// coefficients when the history is not in registers); element k of a lane
+// at [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
 // A batched launch places one layer-model slot per quad after the slices.
 template <class T, int L, int S> struct LaneSlice {
     static constexpr int kCold = 3 * L;                                  // best, outer-start point, start-0 seed
@@ -214,19 +213,13 @@ template <class T, int L, int S> struct LaneSlice {
     static constexpr int kHist = kVec + ((S & kVectorsShared) ? 3 * L : 0);   // history ring (shared history)
     static constexpr int kCoeff = kHist + (history_of(S) == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
     static constexpr int kValues = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
-    static constexpr int kCounters = 5;
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
-    }
-    __device__ __forceinline__ static uint32_t& counter(int k) {
-        return reinterpret_cast<uint32_t*>(solver_smem + value_bytes())[k * kSliceStride + threadIdx.x];
     }
     __host__ __device__ static constexpr size_t value_bytes() {
         return (size_t(kSliceStride) * kValues * sizeof(T) + 15) / 16 * 16;
     }
-    __host__ __device__ static constexpr size_t bytes() {
-        return value_bytes() + (size_t(kSliceStride) * kCounters * sizeof(uint32_t) + 15) / 16 * 16;
-    }
+    __host__ __device__ static constexpr size_t bytes() { return value_bytes(); }
 };
 
 enum : int { kIdle = 0, kOuterEval = 1, kTrial = 2, kAcceptGrad = 3 };
@@ -291,8 +284,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ T& best(int l) const { return Slice::value(l); }
     __device__ __forceinline__ T& ox(int l) const { return Slice::value(L + l); }
     __device__ __forceinline__ T& init(int l) const { return Slice::value(2 * L + l); }
-    __device__ __forceinline__ uint32_t& counter(int k) const { return Slice::counter(k); }
-    __device__ __forceinline__ void count(int k) const { if (a.counters) ++counter(k); }
+    // Work counters go straight to SolveArgs::counters (only when requested).
+    __device__ __forceinline__ uint32_t& counter(int k) const { return a.counters[5 * size_t(gidx) + k]; }
+    __device__ __forceinline__ void count(int k) const { if (a.counters && Q.q == 0) ++counter(k); }
 
     // ------------------------------------------------- image accessors --
     __device__ __forceinline__ const double* image() const {
@@ -828,9 +822,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         }
         have_best = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);
-        if (a.counters)
+        if (a.counters && Q.q == 0)
 #pragma unroll
-            for (int k = 0; k < Slice::kCounters; ++k) counter(k) = 0;
+            for (int k = 0; k < 5; ++k) counter(k) = 0;
     }
 
     // Writes the finished pixel: output (pinned values exactly), FP64
@@ -888,11 +882,6 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             } else {
                 if (stp) stp[i] = miss ? 3 : 0;
                 if (miss && a.miss_list) a.miss_list[atomicAdd(a.miss_count, 1)] = int32_t(gidx);
-            }
-            if (a.counters) {
-                uint32_t* out = a.counters + 5 * size_t(gidx);
-#pragma unroll
-                for (int k = 0; k < Slice::kCounters; ++k) out[k] = counter(k);
             }
         }
     }

@@ -9,7 +9,7 @@ namespace unb {
 // Persistent solve over SolveArgs::n pixels (or SolveArgs::list); the grid
 // is `threads`-wide blocks times the occupancy limit times `sms`.
 // FP32 variants: 0 L-BFGS history in registers; 1, 2 history in shared
-// memory with registers capped for 4, 3 blocks of 128 threads per SM; 3, 4
+// memory with registers capped for 4, 5 blocks of 128 threads per SM; 3, 4
 // history in global memory (SolveArgs::history), registers capped for 5, 6.
 // FP64 variants: 0, 1 history in shared memory with uncapped registers or
 // registers capped for 2 blocks per SM; 2 history in global memory and the

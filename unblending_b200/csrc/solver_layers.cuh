@@ -32,7 +32,7 @@ cudaError_t fp32(int variant, const Models<float>& m, const SolverControls& c, c
     switch (variant) {
     case 0: return go<float, R, kHistRegisters, 1, BATCH>(m, c, a, threads, sms, s);
     case 1: return go<float, R, kHistShared, 4, BATCH>(m, c, a, threads, sms, s);
-    case 2: return go<float, R, kHistShared, 3, BATCH>(m, c, a, threads, sms, s);
+    case 2: return go<float, R, kHistShared, 5, BATCH>(m, c, a, threads, sms, s);
     case 3: return go<float, R, kHistGlobal, 5, BATCH>(m, c, a, threads, sms, s);
     case 4: return go<float, R, kHistGlobal, 6, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;

@@ -223,14 +223,12 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
     return UNBLENDING_OK;
 }
 
-// FP32 kernel variant measured on B200 (1024x1024, 5 layers, FP32 solve
-// times of the first pass / refinement in ms): history in registers 202 / 195,
-// shared history with 4 blocks per SM 194 / 158, 3 blocks 220 / 178,
-// 5 blocks 199 / 173, 6 blocks 205 / 220.
-int default_fp32_variant(int L, bool refine) {
-    (void)L; (void)refine;
-    return 1;
-}
+// FP32 kernel variant measured on B200 (1024x1024, 5 layers, FP32 solve of
+// the first pass / refinement, ms): history in shared memory with registers
+// capped for 4 blocks per SM 56.4 / 62.5, for 5 blocks 54.1 / 73.3 (the
+// refinement kernel spills at that cap). Five 128-thread blocks fit the
+// shared memory (a 44.5 KB slice per block at 5 layers) up to 5 layers.
+int default_fp32_variant(int L, bool refine) { return (!refine && L <= 5) ? 2 : 1; }
 
 // FP64 kernel variant measured on B200 (1024x1024, 5 layers; re-solve of the
 // FP32 misses, first pass / refinement, ms): shared history uncapped 91 / 130;
