@@ -212,7 +212,12 @@ template <class T, int L, int S> struct LaneSlice {
     static constexpr int kVec = kCold;                                   // x, g, d (kVectorsShared)
     static constexpr int kHist = kVec + ((S & kVectorsShared) ? 3 * L : 0);   // history ring (shared history)
     static constexpr int kCoeff = kHist + (history_of(S) == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
-    static constexpr int kValues = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
+    // FP64 kernels with shared vectors evaluate rolled over the layers, with
+    // their per-layer intermediates (trial point, alphas, composite alpha and
+    // colour, trial gradient) in the slice.
+    static constexpr bool kRolledEval = (S & kVectorsShared) != 0 && sizeof(T) == 8;
+    static constexpr int kScratch = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
+    static constexpr int kValues = kScratch + (kRolledEval ? 5 * L : 0);
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
     }
@@ -348,9 +353,47 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     }
 
     // ---------------------------------------------------------- evaluate --
+    // Constraint rows, the AL value and best-point tracking of an evaluation
+    // whose composite ended at alpha Afin and (this lane's channel) colour cfin.
+    __device__ __forceinline__ T residual_value(T energy, T Afin, T cfin, bool need_grad, bool active) {
+        T terms = T(0), norm = T(0);
+        if (colour) {
+            res[0] = cfin - target;
+            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
+            norm = res[0] * res[0];
+        } else if (REFINE) {
+#pragma unroll
+            for (int l = 0; l < R; ++l) {
+                res[l] = tr[l] - ahat[l];
+                terms += madd(T(0.5) * rho * res[l], res[l], -(lam[l] * res[l]));
+                norm = madd(res[l], res[l], norm);
+            }
+        } else {
+            res[0] = Afin - T(1);
+            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
+            norm = res[0] * res[0];
+        }
+        Q.sum2(terms, norm);
+        const T value = energy + terms;
+        if (active) {
+            count(0);
+            if (need_grad) count(1);
+            const bool feasible = norm < tol2;
+            if (finite_(energy) && finite_(norm) &&
+                (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
+                 (!feasible && best_norm >= tol2 && norm < best_norm))) {
+                have_best = true; best_norm = norm; best_energy = energy;
+#pragma unroll
+                for (int l = 0; l < L; ++l) best(l) = tr[l];
+            }
+        }
+        return value;
+    }
+
     // Evaluates the AL value at tr (uniform across the quad), sets res[] and,
     // when need_grad, the gradient slice ng[]. Tracks the best feasible point.
     __device__ __forceinline__ T evaluate(bool need_grad, bool active) {
+        if constexpr (Slice::kRolledEval) return evaluate_rolled(need_grad, active);
         const Models<T>& m = models();
         T al[L], A[L], pc[L];
 #pragma unroll
@@ -392,37 +435,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             }
         }
         if (!REFINE) energy += T(0.01) * asum;
-        T terms = T(0), norm = T(0);
-        if (colour) {
-            res[0] = pc[L - 1] - target;
-            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
-            norm = res[0] * res[0];
-        } else if (REFINE) {
-#pragma unroll
-            for (int l = 0; l < R; ++l) {
-                res[l] = tr[l] - ahat[l];
-                terms += madd(T(0.5) * rho * res[l], res[l], -(lam[l] * res[l]));
-                norm = madd(res[l], res[l], norm);
-            }
-        } else {
-            res[0] = A[L - 1] - T(1);
-            terms = madd(T(0.5) * rho * res[0], res[0], -(lam[0] * res[0]));
-            norm = res[0] * res[0];
-        }
-        Q.sum2(terms, norm);
-        const T value = energy + terms;
-        if (active) {
-            count(0);
-            if (need_grad) count(1);
-            const bool feasible = norm < tol2;
-            if (finite_(energy) && finite_(norm) &&
-                (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
-                 (!feasible && best_norm >= tol2 && norm < best_norm))) {
-                have_best = true; best_norm = norm; best_energy = energy;
-#pragma unroll
-                for (int l = 0; l < L; ++l) best(l) = tr[l];
-            }
-        }
+        const T value = residual_value(energy, A[L - 1], pc[L - 1], need_grad, active);
         if (need_grad) {
             T adj = colour ? rho * res[0] - lam[0] : T(0);
             T adj3 = (!colour && !REFINE) ? rho * res[0] - lam[0] : T(0);
@@ -486,6 +499,108 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 if (!colour) { ng[l] += ga; adj3 = gp; }
             }
             ng[0] += colour ? adj : adj3;
+        }
+        return value;
+    }
+
+    // The same evaluation, rolled over the layers (one copy of each layer's
+    // code, which keeps the FP64 kernels' instruction footprint small), with
+    // the per-layer intermediates in the lane's slice. Same operations in the
+    // same order as evaluate().
+    __device__ __forceinline__ T evaluate_rolled(bool need_grad, bool active) {
+        const Models<T>& m = models();
+        T* sc = &Slice::value(Slice::kScratch);
+        auto TRc = [sc](int l) -> T& { return sc[l * kSliceStride]; };
+        auto AL = [sc](int l) -> T& { return sc[(L + l) * kSliceStride]; };
+        auto AA = [sc](int l) -> T& { return sc[(2 * L + l) * kSliceStride]; };
+        auto PC = [sc](int l) -> T& { return sc[(3 * L + l) * kSliceStride]; };
+        auto NG = [sc](int l) -> T& { return sc[(4 * L + l) * kSliceStride]; };
+#pragma unroll
+        for (int l = 0; l < L; ++l) { TRc(l) = tr[l]; AL(l) = Q.from(tr[l], 3); }
+        T dprev = AL(0), cprev = tr[0];
+        AA(0) = dprev;
+        PC(0) = cprev;
+#pragma unroll 1
+        for (int l = 1; l < L; ++l) {
+            const T av = AL(l), dd = dprev;
+            const T Al = madd(T(m.Z[l]) * dd, T(1) - av, madd(T(m.X[l]) * av, dd, T(m.Y[l]) * av * (T(1) - dd)));
+            const T s = TRc(l), c = cprev;
+            const T pre = madd(T(m.Z[l]) * dd * (T(1) - av), c,
+                               madd(blend(m, l, s, c) * av, dd, T(m.Y[l]) * av * (T(1) - dd) * s));
+            const T pcl = Al > T(1e-12) ? qdiv(pre, Al) : pre;
+            AA(l) = Al;
+            PC(l) = pcl;
+            dprev = Al;
+            cprev = pcl;
+        }
+        T energy = T(0), asum = T(0);
+#pragma unroll 1
+        for (int l = 0; l < L; ++l) {
+            const T all = AL(l);
+            const T mine = colour ? TRc(l) - mean_of(m, l) : T(0);
+            const T d0 = Q.from(mine, 0), d1 = Q.from(mine, 1), d2 = Q.from(mine, 2);
+            const T* P = m.prec[l];
+            const T v0 = madd(P[2], d2, madd(P[0], d0, P[1] * d1));
+            const T v1 = madd(P[5], d2, madd(P[3], d0, P[4] * d1));
+            const T v2 = madd(P[8], d2, madd(P[6], d0, P[7] * d1));
+            const T D = madd(d2, v2, madd(d0, v0, d1 * v1));
+            energy = madd(all, D, energy);
+            asum += all;
+            if (need_grad) {
+                if (colour) {
+                    const T vq = sel3(Q.q, v0, v1, v2);
+                    const T tq = madd(sel3(Q.q, P[6], P[7], P[8]), d2,
+                                      madd(sel3(Q.q, P[0], P[1], P[2]), d0, sel3(Q.q, P[3], P[4], P[5]) * d1));
+                    NG(l) = all * (vq + tq);
+                } else {
+                    NG(l) = D + (REFINE ? T(0) : T(0.01));
+                }
+            }
+        }
+        if (!REFINE) energy += T(0.01) * asum;
+        const T value = residual_value(energy, dprev, cprev, need_grad, active);
+        if (need_grad) {
+            T adj = colour ? rho * res[0] - lam[0] : T(0);
+            T adj3 = (!colour && !REFINE) ? rho * res[0] - lam[0] : T(0);
+            if (REFINE && !colour)
+#pragma unroll
+                for (int l = 0; l < R; ++l) NG(l) += rho * res[l] - lam[l];
+#pragma unroll 1
+            for (int l = L - 1; l > 0; --l) {
+                const T av = AL(l), dd = AA(l - 1), Al = AA(l);
+                const T X = T(m.X[l]), Y = T(m.Y[l]), Z = T(m.Z[l]);
+                const T da = madd(X, dd, Y * (T(1) - dd)) - Z * dd;
+                const T db = madd(Z, T(1) - av, X * av - Y * av);
+                const bool big = Al > T(1e-12);
+                T ga, gp;
+                if (colour) {
+                    const T s = TRc(l), c = PC(l - 1), out = PC(l), v = adj;
+                    T fv, fs, fd;
+                    blend3(m, l, s, c, fv, fs, fd);
+                    const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
+                    const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
+                    const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
+                    const T pd = madd(Z * (T(1) - av), c, fv * av - Y * av * s);
+                    if (big) {
+                        ga = v * ((pa - out * da) / Al);
+                        gp = v * ((pd - out * db) / Al);
+                        NG(l) += v * (ds / Al);
+                        adj = v * (dc / Al);
+                    } else {
+                        ga = v * pa; gp = v * pd;
+                        NG(l) += v * ds;
+                        adj = v * dc;
+                    }
+                } else {
+                    ga = adj3 * da;
+                    gp = adj3 * db;
+                }
+                Q.sum2(ga, gp);
+                if (!colour) { NG(l) += ga; adj3 = gp; }
+            }
+            NG(0) += colour ? adj : adj3;
+#pragma unroll
+            for (int l = 0; l < L; ++l) ng[l] = NG(l);
         }
         return value;
     }

@@ -232,10 +232,10 @@ int default_fp32_variant(int L, bool refine) { return (!refine && L <= 5) ? 2 : 
 
 // FP64 kernel variant measured on B200 (1024x1024, 5 layers; re-solve of the
 // FP32 misses, first pass / refinement, ms): shared history uncapped 91 / 130;
-// global history capped for 3 blocks 76 / 131; global history with x, g, d in
-// shared memory capped for 3 blocks 76 / 122, for 4 blocks 71 / 128. (FP64
-// solve of every pixel: 334 / 321, 320 / 349, 327 / 328, 325 / 365.)
-int default_fp64_variant(bool refine) { return refine ? 2 : 4; }
+// global history with x, g, d and the evaluation's per-layer intermediates in
+// shared memory (evaluation rolled over the layers), capped for 3 blocks:
+// 59 / 83 (FP64 solve of every pixel: 282 / 238, against 342 / 324 uncapped).
+int default_fp64_variant(bool refine) { (void)refine; return 2; }
 int fp64_variant(const unblending_solver_options& so, bool refine) {
     return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
 }
