@@ -83,6 +83,10 @@ enum : int { kHistRegisters = 0, kHistShared = 1, kHistGlobal = 2 };
 // direction d (vectors the evaluation does not touch) in the lane's
 // shared-memory slice instead of registers.
 enum : int { kVectorsShared = 4 };
+// kRolled: the evaluation runs rolled over the layers, its per-layer
+// intermediates in the lane's slice (one copy of each layer's code: a smaller
+// instruction footprint for more shared memory).
+enum : int { kRolled = 8 };
 constexpr int history_of(int storage) { return storage & 3; }
 
 struct Quad {
@@ -212,10 +216,9 @@ template <class T, int L, int S> struct LaneSlice {
     static constexpr int kVec = kCold;                                   // x, g, d (kVectorsShared)
     static constexpr int kHist = kVec + ((S & kVectorsShared) ? 3 * L : 0);   // history ring (shared history)
     static constexpr int kCoeff = kHist + (history_of(S) == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
-    // FP64 kernels with shared vectors evaluate rolled over the layers, with
-    // their per-layer intermediates (trial point, alphas, composite alpha and
-    // colour, trial gradient) in the slice.
-    static constexpr bool kRolledEval = (S & kVectorsShared) != 0 && sizeof(T) == 8;
+    // Rolled evaluation (kRolled): per-layer intermediates (trial point,
+    // alphas, composite alpha and colour, trial gradient) in the slice.
+    static constexpr bool kRolledEval = (S & kRolled) != 0;
     static constexpr int kScratch = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
     static constexpr int kValues = kScratch + (kRolledEval ? 5 * L : 0);
     __device__ __forceinline__ static T& value(int k) {
@@ -573,7 +576,27 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 const T db = madd(Z, T(1) - av, X * av - Y * av);
                 const bool big = Al > T(1e-12);
                 T ga, gp;
-                if (colour) {
+                if constexpr (kFast) {
+                    const T s = TRc(l), c = PC(l - 1), out = PC(l), v = adj;
+                    T fv, fs, fd;
+                    blend3(m, l, s, c, fv, fs, fd);
+                    const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
+                    const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
+                    const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
+                    const T pd = madd(Z * (T(1) - av), c, fv * av - Y * av * s);
+                    const T r = big ? qdiv(T(1), Al) : T(1);
+                    T gs, ad;
+                    if (big) {
+                        ga = v * (madd(-out, da, pa) * r);
+                        gp = v * (madd(-out, db, pd) * r);
+                        gs = v * (ds * r);
+                        ad = v * (dc * r);
+                    } else {
+                        ga = v * pa; gp = v * pd; gs = v * ds; ad = v * dc;
+                    }
+                    if (colour) { NG(l) += gs; adj = ad; }
+                    else { ga = adj3 * da; gp = adj3 * db; }
+                } else if (colour) {
                     const T s = TRc(l), c = PC(l - 1), out = PC(l), v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);

@@ -9,14 +9,16 @@ namespace unb {
 // Persistent solve over SolveArgs::n pixels (or SolveArgs::list); the grid
 // is `threads`-wide blocks times the occupancy limit times `sms`.
 // FP32 variants: 0 L-BFGS history in registers; 1, 2 history in shared
-// memory with registers capped for 4, 5 blocks of 128 threads per SM; 3, 4
-// history in global memory (SolveArgs::history), registers capped for 5, 6.
+// memory with registers capped for 4, 5 blocks of 128 threads per SM; 3 as 1
+// with the evaluation rolled over the layers; 4 history in global memory
+// (SolveArgs::history), evaluation rolled, capped for 5 blocks.
 // FP64 variants: 0, 1 history in shared memory with uncapped registers or
-// registers capped for 2 blocks per SM; 2 history in global memory and the
-// iterate, gradient and direction in shared memory, capped for 3 blocks;
-// 3 history in global memory, capped for 3 blocks; 4 as 2, capped for 4 blocks.
+// registers capped for 2 blocks per SM; 2 history in global memory, the
+// iterate, gradient and direction in shared memory, evaluation rolled, capped
+// for 3 blocks; 3 history in global memory, capped for 3 blocks; 4 as 2,
+// capped for 4 blocks.
 constexpr int kFp32Variants = 5, kFp64Variants = 5;
-inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant >= 3; }
+inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant == 4; }
 // Blocks per SM that a global-history array is sized for (the launch clamps
 // its grid to the array).
 constexpr int kGlobalHistoryBlocksPerSm = 6;

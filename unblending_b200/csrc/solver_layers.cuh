@@ -33,8 +33,8 @@ cudaError_t fp32(int variant, const Models<float>& m, const SolverControls& c, c
     case 0: return go<float, R, kHistRegisters, 1, BATCH>(m, c, a, threads, sms, s);
     case 1: return go<float, R, kHistShared, 4, BATCH>(m, c, a, threads, sms, s);
     case 2: return go<float, R, kHistShared, 5, BATCH>(m, c, a, threads, sms, s);
-    case 3: return go<float, R, kHistGlobal, 5, BATCH>(m, c, a, threads, sms, s);
-    case 4: return go<float, R, kHistGlobal, 6, BATCH>(m, c, a, threads, sms, s);
+    case 3: return go<float, R, kHistShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
+    case 4: return go<float, R, kHistGlobal | kRolled, 5, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -45,9 +45,9 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
     switch (variant) {
     case 0: return go<double, R, kHistShared, 1, BATCH>(m, c, a, threads, sms, s);
     case 1: return go<double, R, kHistShared, 2, BATCH>(m, c, a, threads, sms, s);
-    case 2: return go<double, R, kHistGlobal | kVectorsShared, 3, BATCH>(m, c, a, threads, sms, s);
+    case 2: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 3, BATCH>(m, c, a, threads, sms, s);
     case 3: return go<double, R, kHistGlobal, 3, BATCH>(m, c, a, threads, sms, s);
-    case 4: return go<double, R, kHistGlobal | kVectorsShared, 4, BATCH>(m, c, a, threads, sms, s);
+    case 4: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -223,12 +223,12 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
     return UNBLENDING_OK;
 }
 
-// FP32 kernel variant measured on B200 (1024x1024, 5 layers, FP32 solve of
-// the first pass / refinement, ms): history in shared memory with registers
-// capped for 4 blocks per SM 56.4 / 62.5, for 5 blocks 54.1 / 73.3 (the
-// refinement kernel spills at that cap). Five 128-thread blocks fit the
-// shared memory (a 44.5 KB slice per block at 5 layers) up to 5 layers.
-int default_fp32_variant(int L, bool refine) { return (!refine && L <= 5) ? 2 : 1; }
+// FP32 kernel variant measured on B200 (FP32 solve of the first pass /
+// refinement, ms; 1024x1024, 5 layers | 6 layers with colour noise): history
+// in shared memory, registers capped for 4 blocks per SM 56.6 / 62.7 |
+// 133 / 116; capped for 5 blocks 54.1 / 73.6 | 158 / 181; capped for 4 blocks
+// with the evaluation rolled over the layers 54.3 / 48.6 | 130 / 101.
+int default_fp32_variant(int L, bool refine) { (void)L; (void)refine; return 3; }
 
 // FP64 kernel variant measured on B200 (1024x1024, 5 layers; re-solve of the
 // FP32 misses, first pass / refinement, ms): shared history uncapped 91 / 130;
@@ -806,7 +806,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                         int32_t* d_count = plan->alloc<int32_t>(1);
                         ck(cudaMemcpyAsync(d_sample, sample.data(), S * sizeof(int32_t), cudaMemcpyHostToDevice, s));
                         ck(cudaMemcpyAsync(d_count, &S, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-                        const std::pair<int, int> candidates[4] = {{1, 128}, {0, 128}, {2, 128}, {1, 64}};
+                        const std::pair<int, int> candidates[4] = {{3, 128}, {1, 128}, {2, 128}, {3, 64}};
                         float best_ms = 1e30f;
                         std::pair<int, int> best = candidates[0];
                         for (const auto& cand : candidates) {
