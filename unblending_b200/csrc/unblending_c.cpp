@@ -1163,7 +1163,7 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
             ++t_launches;
         } else {
             int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, false);
-            if (variant_global_history(false, variant)) variant = 1;
+            if (variant_global_history(false, variant)) variant = 3;
             ck(launch_solve_fp32(L, false, variant, make_models<float>(layers, L), ctl32, a, threads, sms, s));
             ++t_launches;
             if (so.resolve_misses) {
