@@ -348,6 +348,17 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         else blend_all_call<T>(m.mode[l], s, d, f, fs, fd);
     }
 
+    // The same, with the FP64 switch inline (the rolled evaluation has one
+    // copy of each layer's code).
+    __device__ __forceinline__ T blend_inline(const Models<T>& m, int l, T s, T d) const {
+        if constexpr (kFast) return blend(m, l, s, d);
+        else return blend_value<T>(m.mode[l], s, d);
+    }
+    __device__ __forceinline__ void blend3_inline(const Models<T>& m, int l, T s, T d, T& f, T& fs, T& fd) const {
+        if constexpr (kFast) blend3(m, l, s, d, f, fs, fd);
+        else blend_all<T>(m.mode[l], s, d, f, fs, fd);
+    }
+
     // sy > 1e-9 sqrt(ss yy) and sy > 0 (augmented_lagrangian.cuh:193,290); the
     // FP32 solver compares squares instead of taking the root.
     __device__ __forceinline__ static bool curvature_ok(T sy, T ss, T yy) {
@@ -529,7 +540,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T Al = madd(T(m.Z[l]) * dd, T(1) - av, madd(T(m.X[l]) * av, dd, T(m.Y[l]) * av * (T(1) - dd)));
             const T s = TRc(l), c = cprev;
             const T pre = madd(T(m.Z[l]) * dd * (T(1) - av), c,
-                               madd(blend(m, l, s, c) * av, dd, T(m.Y[l]) * av * (T(1) - dd) * s));
+                               madd(blend_inline(m, l, s, c) * av, dd, T(m.Y[l]) * av * (T(1) - dd) * s));
             const T pcl = Al > T(1e-12) ? qdiv(pre, Al) : pre;
             AA(l) = Al;
             PC(l) = pcl;
@@ -579,7 +590,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 if constexpr (kFast) {
                     const T s = TRc(l), c = PC(l - 1), out = PC(l), v = adj;
                     T fv, fs, fd;
-                    blend3(m, l, s, c, fv, fs, fd);
+                    blend3_inline(m, l, s, c, fv, fs, fd);
                     const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
                     const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
                     const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
@@ -599,7 +610,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 } else if (colour) {
                     const T s = TRc(l), c = PC(l - 1), out = PC(l), v = adj;
                     T fv, fs, fd;
-                    blend3(m, l, s, c, fv, fs, fd);
+                    blend3_inline(m, l, s, c, fv, fs, fd);
                     const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
                     const T dc = madd(av * dd, fd, Z * dd * (T(1) - av));
                     const T pa = madd(fv, dd, Y * (T(1) - dd) * s) - Z * dd * c;
