@@ -87,43 +87,71 @@ enum : int { kVectorsShared = 4 };
 // intermediates in the lane's slice (one copy of each layer's code: a smaller
 // instruction footprint for more shared memory).
 enum : int { kRolled = 8 };
+// kTriple (refinement only): three lanes per pixel, the colour channels; the
+// pinned alphas need no lane (see Group).
+enum : int { kTriple = 16 };
 constexpr int history_of(int storage) { return storage & 3; }
 
-struct Quad {
+// The lanes of one pixel. G = 4 (a quad, lanes 0..2 colour channels, lane 3
+// the alphas): sums are xor-trees, identical on every lane. G = 3 (the
+// refinement of pinned alphas: colour channels only, 10 pixels per warp,
+// lanes 30-31 idle): sums gather the three values and add them in one fixed
+// order, so every lane holds the identical result.
+template <int G> struct Group {
     unsigned mask;
     int base, q;
-    __device__ __forceinline__ Quad() {
+    bool extra;   // a lane of no group (G = 3: lanes 30 and 31)
+    __device__ __forceinline__ Group() {
         const int lane = threadIdx.x & 31;
-        base = lane & ~3;
-        q = lane & 3;
-        mask = 0xFu << base;
+        base = lane / G * G;
+        q = lane - base;
+        extra = G != 4 && base + G > 32;
+        mask = extra ? 0u : ((1u << G) - 1u) << base;
     }
     template <class T> __device__ __forceinline__ T sum(T v) const {
-        v += __shfl_xor_sync(mask, v, 1);
-        v += __shfl_xor_sync(mask, v, 2);
-        return v;
+        if constexpr (G == 4) {
+            v += __shfl_xor_sync(mask, v, 1);
+            v += __shfl_xor_sync(mask, v, 2);
+            return v;
+        } else {
+            const T a0 = __shfl_sync(mask, v, base), a1 = __shfl_sync(mask, v, base + 1),
+                    a2 = __shfl_sync(mask, v, base + 2);
+            return (a0 + a1) + a2;
+        }
     }
     template <class T> __device__ __forceinline__ void sum2(T& a, T& b) const {
-        a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1);
-        a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2);
+        if constexpr (G == 4) {
+            a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1);
+            a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2);
+        } else { a = sum(a); b = sum(b); }
     }
     template <class T> __device__ __forceinline__ void sum3(T& a, T& b, T& c) const {
-        a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1); c += __shfl_xor_sync(mask, c, 1);
-        a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2); c += __shfl_xor_sync(mask, c, 2);
+        if constexpr (G == 4) {
+            a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1); c += __shfl_xor_sync(mask, c, 1);
+            a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2); c += __shfl_xor_sync(mask, c, 2);
+        } else { a = sum(a); b = sum(b); c = sum(c); }
     }
     template <class T> __device__ __forceinline__ void sum4(T& a, T& b, T& c, T& d) const {
-        a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1);
-        c += __shfl_xor_sync(mask, c, 1); d += __shfl_xor_sync(mask, d, 1);
-        a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2);
-        c += __shfl_xor_sync(mask, c, 2); d += __shfl_xor_sync(mask, d, 2);
+        if constexpr (G == 4) {
+            a += __shfl_xor_sync(mask, a, 1); b += __shfl_xor_sync(mask, b, 1);
+            c += __shfl_xor_sync(mask, c, 1); d += __shfl_xor_sync(mask, d, 1);
+            a += __shfl_xor_sync(mask, a, 2); b += __shfl_xor_sync(mask, b, 2);
+            c += __shfl_xor_sync(mask, c, 2); d += __shfl_xor_sync(mask, d, 2);
+        } else { a = sum(a); b = sum(b); c = sum(c); d = sum(d); }
     }
     template <class T> __device__ __forceinline__ T max(T v) const {
-        v = fmax(v, __shfl_xor_sync(mask, v, 1));
-        v = fmax(v, __shfl_xor_sync(mask, v, 2));
-        return v;
+        if constexpr (G == 4) {
+            v = fmax(v, __shfl_xor_sync(mask, v, 1));
+            v = fmax(v, __shfl_xor_sync(mask, v, 2));
+            return v;
+        } else {
+            const T a0 = __shfl_sync(mask, v, base), a1 = __shfl_sync(mask, v, base + 1),
+                    a2 = __shfl_sync(mask, v, base + 2);
+            return fmax(fmax(a0, a1), a2);
+        }
     }
     template <class T> __device__ __forceinline__ T from(T v, int src) const {
-        return __shfl_sync(mask, v, base | src);
+        return __shfl_sync(mask, v, base + src);
     }
 };
 
@@ -238,13 +266,15 @@ enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart,
 // models are staged in the shared-memory slot that `m` refers to.
 template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSolver {
     static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
+    static constexpr int kLanes = (S & kTriple) ? 3 : 4;   // lanes per pixel
+    static_assert(kLanes == 4 || (REFINE && !BATCH), "three-lane groups serve the refinement only");
     using Slice = LaneSlice<T, L, S>;
     static constexpr int HS = history_of(S);
     static constexpr bool VS = (S & kVectorsShared) != 0;
     const Models<T>* models_;
     const SolverControls& ctl;
     const SolveArgs& a;
-    Quad Q;
+    Group<kLanes> Q;
     bool colour, opaque, smooth;
     T tol2, itol;
 
@@ -258,6 +288,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     mutable T xr_[VS ? 1 : L], gr_[VS ? 1 : L], dr_[VS ? 1 : L];   // x, g, d in registers (!VS)
     T tr[L], ng[L];
     T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
+    // G = 3: every lane's copy of the (pinned) alphas' gradient at x and at the
+    // trial point; they enter only y.y of the curvature pairs.
+    T ga3[kLanes == 3 ? L : 1], na3[kLanes == 3 ? L : 1];
     History<T, L, HS, Slice::kHist> hist;
 
     // Per-quad scalars (uniform within the quad).
@@ -268,7 +301,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 
     __device__ QuadSolver(const Models<T>* models, const SolverControls& c, const SolveArgs& args)
         : models_(models), ctl(c), a(args) {
-        colour = Q.q < 3;
+        colour = kLanes == 3 || Q.q < 3;
         opaque = a.opaque != 0;
         smooth = a.smooth != 0;
         tol2 = T(ctl.outer_tolerance * ctl.outer_tolerance);
@@ -332,6 +365,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const T lv = lo(l), hv = hi(l);
         return lv == hv || (X(l) <= lv && gl > T(0)) || (X(l) >= hv && gl < T(0));
     }
+    // Alpha of layer l at the point whose lane-3 slice is v (G = 4), or the
+    // pinned alpha (G = 3).
+    __device__ __forceinline__ T alpha_at(T v, int l) const {
+        if constexpr (kLanes == 3) return ahat[REFINE ? l : 0];
+        else return Q.from(v, 3);
+    }
     __device__ __forceinline__ T mean_of(const Models<T>& m, int l) const {
         return colour ? sel3(Q.q, m.mean[l][0], m.mean[l][1], m.mean[l][2]) : T(0);
     }
@@ -364,6 +403,21 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ static bool curvature_ok(T sy, T ss, T yy) {
         if constexpr (kFast) return sy > T(0) && sy * sy > T(1e-18) * (ss * yy);
         else return sy > T(1e-9) * dsqrt(ss * yy) && sy > T(0);
+    }
+
+    // G = 3, reverse sweep, layer l: the alpha chain's sensitivities from the
+    // three channels' terms (ga, gp of this lane), summed in the reference's
+    // order (alpha term, then channels 0, 1, 2; pixel_problem.cuh:96-106), on
+    // every lane.
+    __device__ __forceinline__ void alpha_chain(int l, T da, T db, T ga, T gp, T& adj3, T& nal) const {
+        const T a0 = Q.from(ga, 0), a1 = Q.from(ga, 1), a2 = Q.from(ga, 2);
+        const T p0 = Q.from(gp, 0), p1 = Q.from(gp, 1), p2 = Q.from(gp, 2);
+        T ta = adj3 * da, tp = adj3 * db;
+        ta += a0; ta += a1; ta += a2;
+        tp += p0; tp += p1; tp += p2;
+        nal += ta;
+        adj3 = tp;
+        (void)l;
     }
 
     // ---------------------------------------------------------- evaluate --
@@ -411,7 +465,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const Models<T>& m = models();
         T al[L], A[L], pc[L];
 #pragma unroll
-        for (int l = 0; l < L; ++l) al[l] = Q.from(tr[l], 3);
+        for (int l = 0; l < L; ++l) al[l] = alpha_at(tr[l], l);
         A[0] = al[0];
         pc[0] = tr[0];
 #pragma unroll
@@ -446,6 +500,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 } else {
                     ng[l] = D + (REFINE ? T(0) : T(0.01));
                 }
+                if constexpr (kLanes == 3) na3[l] = D;
             }
         }
         if (!REFINE) energy += T(0.01) * asum;
@@ -509,10 +564,15 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     ga = adj3 * da;
                     gp = adj3 * db;
                 }
-                Q.sum2(ga, gp);
-                if (!colour) { ng[l] += ga; adj3 = gp; }
+                if constexpr (kLanes == 4) {
+                    Q.sum2(ga, gp);
+                    if (!colour) { ng[l] += ga; adj3 = gp; }
+                } else {
+                    alpha_chain(l, da, db, ga, gp, adj3, na3[l]);
+                }
             }
             ng[0] += colour ? adj : adj3;
+            if constexpr (kLanes == 3) na3[0] += adj3;
         }
         return value;
     }
@@ -525,12 +585,23 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const Models<T>& m = models();
         T* sc = &Slice::value(Slice::kScratch);
         auto TRc = [sc](int l) -> T& { return sc[l * kSliceStride]; };
-        auto AL = [sc](int l) -> T& { return sc[(L + l) * kSliceStride]; };
+        // G = 4: the alphas of the trial point; G = 3: the slot holds the alpha
+        // gradient (NA) and the pinned alphas are read from the filter targets.
+        auto ALs = [sc](int l) -> T& { return sc[(L + l) * kSliceStride]; };
+        const size_t npx = pixels(), pix = size_t(pixel);
+        auto AL = [&](int l) -> T {
+            if constexpr (kLanes == 3) return (opaque && l == 0) ? T(1) : T(a.targets[size_t(l) * npx + pix]);
+            else return ALs(l);
+        };
         auto AA = [sc](int l) -> T& { return sc[(2 * L + l) * kSliceStride]; };
         auto PC = [sc](int l) -> T& { return sc[(3 * L + l) * kSliceStride]; };
         auto NG = [sc](int l) -> T& { return sc[(4 * L + l) * kSliceStride]; };
+        auto NA = [sc](int l) -> T& { return sc[(L + l) * kSliceStride]; };   // G = 3: alpha gradient
 #pragma unroll
-        for (int l = 0; l < L; ++l) { TRc(l) = tr[l]; AL(l) = Q.from(tr[l], 3); }
+        for (int l = 0; l < L; ++l) {
+            TRc(l) = tr[l];
+            if constexpr (kLanes == 4) ALs(l) = alpha_at(tr[l], l);
+        }
         T dprev = AL(0), cprev = tr[0];
         AA(0) = dprev;
         PC(0) = cprev;
@@ -569,6 +640,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 } else {
                     NG(l) = D + (REFINE ? T(0) : T(0.01));
                 }
+                if constexpr (kLanes == 3) NA(l) = D;
             }
         }
         if (!REFINE) energy += T(0.01) * asum;
@@ -629,12 +701,20 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     ga = adj3 * da;
                     gp = adj3 * db;
                 }
-                Q.sum2(ga, gp);
-                if (!colour) { NG(l) += ga; adj3 = gp; }
+                if constexpr (kLanes == 4) {
+                    Q.sum2(ga, gp);
+                    if (!colour) { NG(l) += ga; adj3 = gp; }
+                } else {
+                    alpha_chain(l, da, db, ga, gp, adj3, NA(l));
+                }
             }
             NG(0) += colour ? adj : adj3;
+            if constexpr (kLanes == 3) NA(0) += adj3;
 #pragma unroll
             for (int l = 0; l < L; ++l) ng[l] = NG(l);
+            if constexpr (kLanes == 3)
+#pragma unroll
+                for (int l = 0; l < L; ++l) na3[l] = NA(l);
         }
         return value;
     }
@@ -763,7 +843,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             // Move Dodge/Burn sources into the unsaturated branch.
             T av[L];
 #pragma unroll
-            for (int l = 0; l < L; ++l) av[l] = Q.from(X(l), 3);
+            for (int l = 0; l < L; ++l) av[l] = alpha_at(X(l), l);
             T dest = X(0), da = av[0];
 #pragma unroll
             for (int l = 1; l < L; ++l) {
@@ -893,6 +973,14 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
         }
         Q.sum3(sy, ss, yy);
+        if constexpr (kLanes == 3) {
+            // The pinned alphas do not move, but their gradient change counts
+            // in y.y (the same on every lane).
+            T ya = T(0);
+#pragma unroll
+            for (int l = 0; l < L; ++l) { const T dy = na3[l] - ga3[l]; ya = madd(dy, dy, ya); }
+            yy += ya;
+        }
         mm = Q.max(mm);
         const T r = qdiv(T(1), sy);
         if (curvature_ok(sy, ss, yy) && finite_(r)) {
@@ -902,6 +990,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const T delta = fabs(f - cand), size = T(0.5) * (fabs(f) + fabs(cand));
 #pragma unroll
         for (int l = 0; l < L; ++l) { X(l) = tr[l]; G(l) = ng[l]; }
+        if constexpr (kLanes == 3)
+#pragma unroll
+            for (int l = 0; l < L; ++l) ga3[l] = na3[l];
 #pragma unroll
         for (int q = 0; q < R; ++q) resx[q] = res[q];
         f = cand;
@@ -916,6 +1007,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             f = value;
 #pragma unroll
             for (int l = 0; l < L; ++l) G(l) = ng[l];
+            if constexpr (kLanes == 3)
+#pragma unroll
+                for (int l = 0; l < L; ++l) ga3[l] = na3[l];
 #pragma unroll
             for (int q = 0; q < R; ++q) resx[q] = res[q];
             oldnorm = Q.sum(own_norm(res));
@@ -990,15 +1084,17 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             if (REFINE && smooth && colour && l == 0) v = a.targets[(size_t(L) + Q.q) * n + i];
             if (!REFINE && opaque && !colour && l == 0) v = 1.0;
             outp[(size_t(l) * n + i) * 4 + Q.q] = v;
+            if (kLanes == 3 && Q.q == 0)   // the pinned alpha (no alpha lane)
+                outp[(size_t(l) * n + i) * 4 + 3] = (opaque && l == 0) ? 1.0 : a.targets[size_t(l) * n + i];
             if (l == 0) v0 = v;
         }
         // FP64 constraint check of the written point (solver_workspace.cuh:18-38),
         // one layer per trip, reading back the values just written.
-        double A = Q.from(v0, 3), c = v0;
+        double A = kLanes == 3 ? (opaque ? 1.0 : a.targets[i]) : Q.from(v0, 3), c = v0;
 #pragma unroll 1
         for (int l = 1; l < L; ++l) {
             const double s = outp[(size_t(l) * n + i) * 4 + Q.q];
-            const double al = Q.from(s, 3), dd = A;
+            const double al = kLanes == 3 ? a.targets[size_t(l) * n + i] : Q.from(s, 3), dd = A;
             const double Al = double(m.X[l]) * al * dd + double(m.Y[l]) * al * (1.0 - dd) +
                               double(m.Z[l]) * dd * (1.0 - al);
             const double pre = blend_value<double>(m.mode[l], s, c) * al * dd + double(m.Y[l]) * al * (1.0 - dd) * s +
@@ -1076,8 +1172,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     // ------------------------------------------------------------- loop --
     __device__ void run() {
         const int total = a.list ? *a.list_count : a.n;
-        bool live = true;
-        int act = aFetch;
+        bool live = !Q.extra;            // lanes of no group stay idle throughout
+        int act = live ? aFetch : aEval;
         for (;;) {
             while (act != aEval) {
                 switch (act) {
@@ -1094,7 +1190,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             if (__all_sync(0xffffffffu, !live)) break;
             const bool need_grad = phase == kOuterEval || phase == kAcceptGrad ||
                                    (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial);
-            const T value = evaluate(need_grad && live, live);
+            const T value = Q.extra ? T(0) : evaluate(need_grad && live, live);
             act = live ? after_evaluation(value, need_grad) : aEval;
         }
     }

@@ -17,7 +17,10 @@ namespace unb {
 // iterate, gradient and direction in shared memory, evaluation rolled, capped
 // for 3 blocks; 3 history in global memory, capped for 3 blocks; 4 as 2,
 // capped for 4 blocks.
-constexpr int kFp32Variants = 5, kFp64Variants = 5;
+// Variant 5 (FP32 and FP64): the refinement with three lanes per pixel (its
+// alphas are pinned, so no alpha lane: 10 pixels per warp), FP32 as 3 and
+// FP64 as 2 otherwise; first passes run variant 3 / 2 for it.
+constexpr int kFp32Variants = 6, kFp64Variants = 6;
 inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant == 4; }
 // Blocks per SM that a global-history array is sized for (the launch clamps
 // its grid to the array).

@@ -35,6 +35,9 @@ cudaError_t fp32(int variant, const Models<float>& m, const SolverControls& c, c
     case 2: return go<float, R, kHistShared, 5, BATCH>(m, c, a, threads, sms, s);
     case 3: return go<float, R, kHistShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
     case 4: return go<float, R, kHistGlobal | kRolled, 5, BATCH>(m, c, a, threads, sms, s);
+    case 5:   // three lanes per pixel where the alphas are pinned (refinement), else variant 3
+        if constexpr (R && !BATCH) return go<float, R, kHistShared | kRolled | kTriple, 4, BATCH>(m, c, a, threads, sms, s);
+        else return go<float, R, kHistShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -48,6 +51,10 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
     case 2: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 3, BATCH>(m, c, a, threads, sms, s);
     case 3: return go<double, R, kHistGlobal, 3, BATCH>(m, c, a, threads, sms, s);
     case 4: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
+    case 5:   // three lanes per pixel where the alphas are pinned (refinement), else variant 2
+        if constexpr (R && !BATCH)
+            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple, 3, BATCH>(m, c, a, threads, sms, s);
+        else return go<double, R, kHistGlobal | kVectorsShared | kRolled, 3, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
