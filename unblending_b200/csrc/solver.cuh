@@ -90,6 +90,10 @@ enum : int { kRolled = 8 };
 // kTriple (refinement only): three lanes per pixel, the colour channels; the
 // pinned alphas need no lane (see Group).
 enum : int { kTriple = 16 };
+// kColdGlobal (with global history): the cold values (best point, outer-step
+// start, start-0 seed) follow the history in the lane's global array, which
+// shrinks the shared-memory slice.
+enum : int { kColdGlobal = 32 };
 constexpr int history_of(int storage) { return storage & 3; }
 
 // The lanes of one pixel. G = 4 (a quad, lanes 0..2 colour channels, lane 3
@@ -240,7 +244,7 @@ template <class T, int L, int BASE> struct History<T, L, kHistGlobal, BASE> {
 // at [k * kSliceStride + threadIdx.x] (consecutive lanes, consecutive words).
 // A batched launch places one layer-model slot per quad after the slices.
 template <class T, int L, int S> struct LaneSlice {
-    static constexpr int kCold = 3 * L;                                  // best, outer-start point, start-0 seed
+    static constexpr int kCold = (S & kColdGlobal) ? 0 : 3 * L;          // best, outer-start point, start-0 seed
     static constexpr int kVec = kCold;                                   // x, g, d (kVectorsShared)
     static constexpr int kHist = kVec + ((S & kVectorsShared) ? 3 * L : 0);   // history ring (shared history)
     static constexpr int kCoeff = kHist + (history_of(S) == kHistShared ? 2 * kHistory * L : 0);   // two-loop coefficients
@@ -322,9 +326,17 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ T& X(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + l); else return xr_[l]; }
     __device__ __forceinline__ T& G(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + L + l); else return gr_[l]; }
     __device__ __forceinline__ T& D(int l) const { if constexpr (VS) return Slice::value(Slice::kVec + 2 * L + l); else return dr_[l]; }
-    __device__ __forceinline__ T& best(int l) const { return Slice::value(l); }
-    __device__ __forceinline__ T& ox(int l) const { return Slice::value(L + l); }
-    __device__ __forceinline__ T& init(int l) const { return Slice::value(2 * L + l); }
+    __device__ __forceinline__ T& cold(int k) const {
+        if constexpr ((S & kColdGlobal) != 0) {
+            static_assert(HS == kHistGlobal, "global cold values follow a global history");
+            return hist.base[size_t(2 * kHistory * L + k) * hist.lanes];
+        } else {
+            return Slice::value(k);
+        }
+    }
+    __device__ __forceinline__ T& best(int l) const { return cold(l); }
+    __device__ __forceinline__ T& ox(int l) const { return cold(L + l); }
+    __device__ __forceinline__ T& init(int l) const { return cold(2 * L + l); }
     // Work counters go straight to SolveArgs::counters (only when requested).
     __device__ __forceinline__ uint32_t& counter(int k) const { return a.counters[5 * size_t(gidx) + k]; }
     __device__ __forceinline__ void count(int k) const { if (a.counters && Q.q == 0) ++counter(k); }

@@ -15,8 +15,9 @@ namespace unb {
 // FP64 variants: 0, 1 history in shared memory with uncapped registers or
 // registers capped for 2 blocks per SM; 2 history in global memory, the
 // iterate, gradient and direction in shared memory, evaluation rolled, capped
-// for 3 blocks; 3 history in global memory, capped for 3 blocks; 4 as 2,
-// capped for 4 blocks.
+// for 3 blocks; 3 as 2 with the cold values (best point, outer-step start,
+// start seed) in the global array too, capped for 4 blocks; 4 as 3 with three
+// lanes per pixel in the refinement.
 // Variant 5 (FP32 and FP64): the refinement with three lanes per pixel (its
 // alphas are pinned, so no alpha lane: 10 pixels per warp), FP32 as 3 and
 // FP64 as 2 otherwise; first passes run variant 3 / 2 for it.

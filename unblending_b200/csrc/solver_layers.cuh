@@ -49,8 +49,11 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
     case 0: return go<double, R, kHistShared, 1, BATCH>(m, c, a, threads, sms, s);
     case 1: return go<double, R, kHistShared, 2, BATCH>(m, c, a, threads, sms, s);
     case 2: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 3, BATCH>(m, c, a, threads, sms, s);
-    case 3: return go<double, R, kHistGlobal, 3, BATCH>(m, c, a, threads, sms, s);
-    case 4: return go<double, R, kHistGlobal | kVectorsShared | kRolled, 4, BATCH>(m, c, a, threads, sms, s);
+    case 3: return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal, 4, BATCH>(m, c, a, threads, sms, s);
+    case 4:   // as 3, three lanes per pixel where the alphas are pinned
+        if constexpr (R && !BATCH)
+            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal | kTriple, 4, BATCH>(m, c, a, threads, sms, s);
+        else return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal, 4, BATCH>(m, c, a, threads, sms, s);
     case 5:   // three lanes per pixel where the alphas are pinned (refinement), else variant 2
         if constexpr (R && !BATCH)
             return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple, 3, BATCH>(m, c, a, threads, sms, s);

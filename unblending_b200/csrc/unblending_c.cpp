@@ -239,7 +239,10 @@ int default_fp32_variant(int L, bool refine) { (void)L; return refine ? 5 : 3; }
 // 59 / 83 (FP64 solve of every pixel: 282 / 238, against 342 / 324 uncapped).
 // The refinement as 2 with three lanes per pixel (variant 5): re-solve 78.6 ->
 // 66.2 ms, FP64 solve of every pixel 221 -> 191 ms.
-int default_fp64_variant(bool refine) { return refine ? 5 : 2; }
+// First passes with the cold values in the global array too (variant 3, a
+// smaller shared slice for 4 blocks per SM): re-solve 60.6 -> 53.0 ms, FP64 solve
+// of every pixel 292 -> 248 ms (for the refinement it gains nothing).
+int default_fp64_variant(bool refine) { return refine ? 5 : 3; }
 int fp64_variant(const unblending_solver_options& so, bool refine) {
     return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
 }
@@ -247,7 +250,8 @@ int fp64_variant(const unblending_solver_options& so, bool refine) {
 // Bytes of a global-memory L-BFGS history array for L layers and values of
 // `elem` bytes, sized for kGlobalHistoryBlocksPerSm blocks on every SM.
 size_t history_lanes(int sms) { return size_t(kGlobalHistoryBlocksPerSm) * sms * kSliceStride; }
-size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * 2 * kHistory * L * elem; }
+// (the history, then the cold values of the variants that keep them there).
+size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * (2 * kHistory + 3) * L * elem; }
 
 // Points `a` at a history array when the kernel variant keeps its history in
 // global memory.
