@@ -200,3 +200,40 @@ def test_device_entry_points_match_host(cuda):
     torch.cuda.synchronize()
     href, _, _, _ = cuda.refine_ex(wl.image, host, wl.layers, smooth=True)
     assert np.array_equal(d_ref.cpu().numpy().reshape(href.shape), href)
+
+
+REFINE_CASES = [
+    # (modes, comp, opaque, smooth)
+    ([0], syn.SOURCE_OVER, True, False),
+    ([0, 1], syn.SOURCE_OVER, True, True),
+    ([0, 1, 2, 3, 9, 5], syn.SOURCE_OVER, True, True),
+    ([0, 6, 7, 9, 1, 2, 8, 11], syn.SOURCE_OVER, True, False),
+    ([0, 1, 2], syn.PLUS, False, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(REFINE_CASES)))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_refinement_three_lane_kernels_match_quad_kernels(cuda, case, precision):
+    """The refinement pins the alphas, so its default kernels run three lanes
+    per pixel; they must give the four-lane kernels' results (same method,
+    same operations) and match the oracle like them."""
+    modes, comp, opaque, smooth = REFINE_CASES[case]
+    wl = syn.generate(20, 18, modes, (4.0, 10.0), seed=300 + case, comp=comp)
+    L = len(modes)
+    first, _ = oracle_unmix(wl, opaque=opaque)
+    quad = dict(kernel_variant=3, fp64_variant=2)
+    triple = dict(kernel_variant=5, fp64_variant=5)
+    outs = []
+    for kv in (quad, triple):
+        out, status, _, _ = cuda.refine_ex(wl.image, first, wl.layers, opaque=opaque, smooth=smooth,
+                                           solver=solver(cuda, precision, radius=3, **kv))
+        outs.append((out, status))
+    (q, qs), (t, ts) = outs
+    same = np.mean(np.abs(q - t).reshape(L, -1, 4).max(axis=(0, 2)) <= 1e-12)
+    print("refine case", case, "precision", precision, "identical pixels", same)
+    assert same >= 0.995
+    assert np.mean(qs == ts) >= 0.995
+    rref, _, _ = oracle_refine(wl, first, opaque=opaque, smooth=smooth, radius=3)
+    r = report(t, rref, wl.layers, True)
+    assert r["frac_rgba_1e-3"] >= (PIXEL_FRACTION if precision == 1 else FP32_RGBA_FLOOR), r
