@@ -153,6 +153,25 @@ def evaluation_flops(L: int, modes: list[int]) -> tuple[float, float]:
     return val, grad
 
 
+ITERATION_EDGES = [0, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096]
+
+
+def iteration_histogram(c):
+    """Per-pixel work of one pass from its (n, 5) counters: a histogram of the
+    L-BFGS iterations a pixel took over all its outer steps (bins
+    [edge_k, edge_k+1), the last open), the outer-step counts, and quantiles.
+    A pixel that the FP32 solve missed carries the counts of its FP64
+    re-solve, the solve that produced its output."""
+    it, outer = c[:, 2], c[:, 4]
+    bins = ITERATION_EDGES + [int(max(it.max(), ITERATION_EDGES[-1])) + 1]
+    counts, _ = np.histogram(it, bins=bins)
+    q = np.quantile(it, [0.5, 0.9, 0.99, 0.999])
+    return {"iterations": {"edges": ITERATION_EDGES, "counts": counts.tolist(),
+                           "p50": float(q[0]), "p90": float(q[1]), "p99": float(q[2]), "p99.9": float(q[3]),
+                           "max": int(it.max()), "mean": float(it.mean())},
+            "outer_steps": {str(k): int(v) for k, v in enumerate(np.bincount(outer)) if v}}
+
+
 # ------------------------------------------------------------ reference --
 def cpu_reference(wl, first_gpu, finals, threads, sample_idx):
     """The reference's CPU implementation on this host: its FP64 solver
@@ -379,6 +398,7 @@ def b200_arm(args):
         warm = {"value": dist.throughput(n, wms, "cuda"), "ms_per_step": dist.reduce_max(wms, "cuda"),
                 "speedup_vs_plain": ms / wms, "training": training,
                 "unmix_counters_mean": wc1.mean(0).tolist(),
+                "unmix_iteration_histogram": iteration_histogram(wc1),
                 "stages_ms": {"unmix_solve": ws1["ms_solve"], "unmix_resolve_fp64": ws1["ms_resolve"],
                               "filter": ws2["ms_filter"], "refine_solve": ws2["ms_solve"],
                               "refine_resolve_fp64": ws2["ms_resolve"]},
@@ -462,6 +482,7 @@ def b200_arm(args):
                    "refine_failed": s2["failed"]},
         "counters_mean": {"unmix": c1.mean(0).tolist(), "refine": c2.mean(0).tolist(),
                           "fields": ["values", "gradients", "iterations", "line_search_trials", "outer"]},
+        "iteration_histogram": {"unmix": iteration_histogram(c1), "refine": iteration_histogram(c2)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": PEAK_FP32_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / PEAK_FP32_TFLOPS, "traffic": SOLVE_TRAFFIC_BYTES_PER_PIXEL * n,
                      "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz); MEASURED_PEAKS.json has no FP32 figure",

@@ -52,6 +52,30 @@ def test_unmix_matches_oracle_rgb256_l3(cuda, precision):
 
 
 @pytest.mark.parametrize("precision", [1, 0])
+def test_rgb256_l3_full_image_two_passes(cuda, precision):
+    """The whole 256x256 three-layer image (normal, multiply, screen) through
+    the colour unmixing and the refinement (guided filter r = 4, eps = 1e-4),
+    each pass against the oracle's pass from the same input."""
+    wl = syn.workload("rgb256_l3")
+    assert (wl.width, wl.height, len(wl.layers)) == (256, 256, 3)
+    ref1, _ = oracle_unmix(wl)
+    so = solver(cuda, precision, radius=4)
+    first, st1, _, s1 = cuda.unmix_ex(wl.image, wl.layers, solver=so)
+    r1 = report(first, ref1, wl.layers, False)
+    ref2, _, _ = oracle_refine(wl, first, smooth=True, radius=4)
+    final, st2, _, s2 = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so)
+    r2 = report(final, ref2, wl.layers, True)
+    print("rgb256_l3 full", "fp64" if precision else "fp32", r1, r2, s1, s2)
+    assert s2["radius"] == 4
+    assert int((st1 == 3).sum()) == s1["failed"] and int((st2 == 3).sum()) == s2["failed"]
+    for r in (r1, r2):
+        if precision == 1:
+            assert r["frac_rgba_1e-3"] >= PIXEL_FRACTION and r["frac_objective"] >= PIXEL_FRACTION
+        else:
+            assert r["frac_rgba_1e-3"] >= FP32_RGBA_FLOOR and r["frac_objective"] >= FP32_OBJECTIVE_FLOOR
+
+
+@pytest.mark.parametrize("precision", [1, 0])
 def test_refine_matches_oracle_rgb256_l3(cuda, precision):
     wl = syn.workload("rgb256_l3", 96, 96)
     first, _ = oracle_unmix(wl)
