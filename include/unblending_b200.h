@@ -38,22 +38,29 @@ typedef struct unblending_solver_options {
     double inner_tolerance;     /* default 5e-3 */
     double outer_tolerance;     /* feasibility tolerance on |C|, default 5e-3 */
     int32_t threads_per_block;  /* 0 selects the tuned default */
-    int32_t kernel_variant;     /* FP32 solve: -1 tuned default, 0 history in registers, 1/2 in shared memory
-                                   with registers capped for 4/3 blocks per SM, 3/4 in global memory capped
-                                   for 5/6 blocks per SM */
+    int32_t kernel_variant;     /* FP32 solve: -1 tuned default; 0 history in registers; 1/2 history in shared
+                                   memory with registers capped for 4/5 blocks per SM; 3 as 1 with the evaluation
+                                   rolled over the layers; 4 history in global memory, rolled, 5 blocks per SM;
+                                   5 as 3, with three lanes per pixel where the alphas are pinned (refinement) */
     const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start.
                                    With FP32 precision and resolve_misses, pixels the learned start leaves
                                    unsolved get the plain FP32 solve from the reference's start, and what
                                    that misses the FP64 re-solve (the plain path's fallback). */
     int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default; history in shared memory with 0
-                                   uncapped registers, 1/2 capped for 2/3 blocks per SM; history in global
-                                   memory with 3/4 capped for 3/4 blocks per SM */
+                                   uncapped registers, 1 capped for 2 blocks per SM; 2 history in global memory,
+                                   x/g/d in shared memory, evaluation rolled, 3 blocks per SM; 3 as 2 with the
+                                   start and bounds in global memory, 4 blocks per SM; 4/5 as 3/2 with three
+                                   lanes per pixel where the alphas are pinned (refinement) */
     int32_t fp32_outer;         /* FP32 precision with resolve_misses: outer steps of the FP32 solve before a
                                    pixel is left to the FP64 re-solve (default 12; 0 = outer) */
+    int32_t gradient_quorum;    /* scheduling of the pixels of one warp: an evaluation with a gradient runs when
+                                   at least gradient_quorum/8 of the warp's pixels need one (or none needs a
+                                   value alone); the others wait one evaluation. 0 = never wait. Results do not
+                                   depend on it. Default 3, range 0..8 */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 12 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 12, 3 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

@@ -261,3 +261,21 @@ def test_refinement_three_lane_kernels_match_quad_kernels(cuda, case, precision)
     rref, _, _ = oracle_refine(wl, first, opaque=opaque, smooth=smooth, radius=3)
     r = report(t, rref, wl.layers, True)
     assert r["frac_rgba_1e-3"] >= (PIXEL_FRACTION if precision == 1 else FP32_RGBA_FLOOR), r
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_warp_scheduling_quorum_leaves_results_unchanged(cuda, precision):
+    """Pixels of a warp that need a gradient (or, in FP64, a new direction)
+    may wait for others to run it together; each pixel's own sequence of
+    operations is unchanged, so both passes are bit-identical for every
+    quorum, including no waiting at all."""
+    wl = syn.generate(64, 48, [0, 1, 2, 3, 9], (4.0, 16.0), seed=77)
+    outs = []
+    for q in (0, 3, 8):
+        so = solver(cuda, precision, radius=3, gradient_quorum=q)
+        first, st1, c1, _ = cuda.unmix_ex(wl.image, wl.layers, solver=so, with_counters=True)
+        final, st2, c2, _ = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so, with_counters=True)
+        outs.append((first, st1, c1, final, st2, c2))
+    for other in outs[1:]:
+        for a, b in zip(outs[0], other):
+            assert np.array_equal(a, b)

@@ -61,6 +61,8 @@ struct SolverControls {
     int inner = 256, outer = 22, starts = 1;
     double inner_tolerance = 5e-3, outer_tolerance = 5e-3;
     int gradient_on_first_trial = 1;   // fuse the first line-search trial's gradient
+    int gradient_quorum = 3;           // eighths of a warp's live pixels that start a gradient evaluation
+    int direction_quorum = 0;          // eighths of a warp's live pixels that start a new direction (0 = no wait)
 };
 
 // One image of a batched first pass: its pixels occupy global queue indices

@@ -1186,24 +1186,55 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const int total = a.list ? *a.list_count : a.n;
         bool live = !Q.extra;            // lanes of no group stay idle throughout
         int act = live ? aFetch : aEval;
+        const int gq = ctl.gradient_quorum, bq = ctl.direction_quorum;
         for (;;) {
-            while (act != aEval) {
-                switch (act) {
-                case aBeginIter: act = begin_iteration(); break;
-                case aNextTrial: act = next_trial(); break;
-                case aAccept: act = accept(); break;
-                case aEndOuter: act = end_outer(); break;
-                case aBeginStart: act = begin_start(); break;
-                case aBeginOuter: act = begin_outer(); break;
-                case aFinish: store(false); act = aFetch; break;
-                default: act = fetch(total, live); break;
+            // Pixels of the warp that reach a new quasi-Newton direction
+            // (begin_iteration, the two-loop recursion) run it together: while
+            // fewer than direction_quorum/8 of the live pixels are there (and
+            // some are ready to evaluate), they wait one evaluation. A waiting
+            // pixel's evaluate() is inactive at its accepted point, which
+            // recomputes the residuals of that point unchanged.
+            bool allow_bi = bq == 0;
+            for (;;) {
+                while (act != aEval && (allow_bi || act != aBeginIter)) {
+                    switch (act) {
+                    case aBeginIter: act = begin_iteration(); break;
+                    case aNextTrial: act = next_trial(); break;
+                    case aAccept: act = accept(); break;
+                    case aEndOuter: act = end_outer(); break;
+                    case aBeginStart: act = begin_start(); break;
+                    case aBeginOuter: act = begin_outer(); break;
+                    case aFinish: store(false); act = aFetch; break;
+                    default: act = fetch(total, live); break;
+                    }
                 }
+                if (allow_bi) break;
+                const int nb = __popc(__ballot_sync(0xffffffffu, act == aBeginIter));
+                if (nb == 0) break;
+                const int nl = __popc(__ballot_sync(0xffffffffu, live));
+                if (nb < nl && 8 * nb < bq * nl) break;
+                allow_bi = true;
             }
             if (__all_sync(0xffffffffu, !live)) break;
-            const bool need_grad = phase == kOuterEval || phase == kAcceptGrad ||
-                                   (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial);
-            const T value = Q.extra ? T(0) : evaluate(need_grad && live, live);
-            act = live ? after_evaluation(value, need_grad) : aEval;
+            const bool ready = live && act == aEval;
+            const bool need_grad = ready && (phase == kOuterEval || phase == kAcceptGrad ||
+                                             (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial));
+            // The warp runs the gradient part of an evaluation if any of its
+            // pixels needs it, with the others masked off. While fewer than
+            // gradient_quorum/8 of the live pixels need a gradient (and some
+            // need a value alone), those pixels wait: this evaluation is
+            // value-only, and they evaluate with the next quorum. A waiting
+            // pixel's evaluate() is inactive and recomputes the residuals of
+            // its unchanged trial point, which its own evaluation then
+            // recomputes identically, so its results do not change.
+            bool go = ready;
+            if (gq > 0) {
+                const int ng = __popc(__ballot_sync(0xffffffffu, need_grad));
+                const int nr = __popc(__ballot_sync(0xffffffffu, ready));
+                if (ng < nr && 8 * ng < gq * nr) go = ready && !need_grad;
+            }
+            const T value = Q.extra ? T(0) : evaluate(need_grad && go, go);
+            if (go) act = after_evaluation(value, need_grad);
         }
     }
 };

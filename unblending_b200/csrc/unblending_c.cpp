@@ -218,7 +218,8 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
         (out.threads_per_block != 0 && (out.threads_per_block % 32 != 0 || out.threads_per_block < 32 ||
                                         out.threads_per_block > 128)) ||
         out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
-        out.fp64_variant >= kFp64Variants || out.fp32_outer < 0)
+        out.fp64_variant >= kFp64Variants || out.fp32_outer < 0 || out.gradient_quorum < 0 ||
+        out.gradient_quorum > 8)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -265,6 +266,12 @@ SolverControls controls(const unblending_solver_options& so) {
     SolverControls c;
     c.inner = so.inner; c.outer = so.outer; c.starts = so.starts;
     c.inner_tolerance = so.inner_tolerance; c.outer_tolerance = so.outer_tolerance;
+    c.gradient_quorum = so.gradient_quorum;
+    // Waiting for a quorum at the direction step pays in the FP64 solve of
+    // every pixel (1024x1024, 5 layers: 211 -> 191 ms first pass, 203 -> 177
+    // refinement) but not in the FP32 solve (50 -> 52 ms) or in the FP64
+    // re-solve of the FP32 misses (44 -> 45 ms).
+    c.direction_quorum = so.precision == UNBLENDING_PRECISION_FP64 ? 3 : 0;
     return c;
 }
 
