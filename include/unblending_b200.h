@@ -52,7 +52,8 @@ typedef struct unblending_solver_options {
                                    start and bounds in global memory, 4 blocks per SM; 4/5 as 3/2 with three
                                    lanes per pixel where the alphas are pinned (refinement) */
     int32_t fp32_outer;         /* FP32 precision with resolve_misses: outer steps of the FP32 solve before a
-                                   pixel is left to the FP64 re-solve (default 12; 0 = outer) */
+                                   pixel is left to the FP64 re-solve (default 9; 0 = outer);
+                                   a pixel stopped there unconverged is always re-solved */
     int32_t gradient_quorum;    /* scheduling of the pixels of one warp: an evaluation with a gradient runs when
                                    at least gradient_quorum/8 of the warp's pixels need one (or none needs a
                                    value alone); the others wait one evaluation. 0 = never wait. Results do not
@@ -60,7 +61,7 @@ typedef struct unblending_solver_options {
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 12, 3 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 9, 3 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

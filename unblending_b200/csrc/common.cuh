@@ -63,6 +63,7 @@ struct SolverControls {
     int gradient_on_first_trial = 1;   // fuse the first line-search trial's gradient
     int gradient_quorum = 3;           // eighths of a warp's live pixels that start a gradient evaluation
     int direction_quorum = 0;          // eighths of a warp's live pixels that start a new direction (0 = no wait)
+    int cap_is_miss = 0;               // a pixel that reaches the outer cap unconverged is a miss
 };
 
 // One image of a batched first pass: its pixels occupy global queue indices

@@ -302,6 +302,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     T rho, f, oldnorm, step, slope, cand;
     T best_norm, best_energy;
     bool have_best;
+    bool capped;     // stopped unconverged at a shortened outer cap (counts as a miss)
 
     __device__ QuadSolver(const Models<T>* models, const SolverControls& c, const SolveArgs& args)
         : models_(models), ctl(c), a(args) {
@@ -909,9 +910,15 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 #pragma unroll
         for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion = madd(dl, dl, motion); }
         motion = Q.sum(motion);
-        if (!(motion < tol2 && feasible) && outer + 1 < ctl.outer) {
-            ++outer;
-            return aBeginOuter;
+        if (!(motion < tol2 && feasible)) {
+            if (outer + 1 < ctl.outer) {
+                ++outer;
+                return aBeginOuter;
+            }
+            // A shortened FP32 solve (the FP64 re-solve behind it) hands an
+            // unconverged pixel over whatever its best point: the re-solve
+            // gives it the method's own result.
+            if (ctl.cap_is_miss) { capped = true; return aFinish; }
         }
         if (start + 1 < ctl.starts) {
             ++start;
@@ -1076,6 +1083,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             init(l) = v;
         }
         have_best = false;
+        capped = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);
         if (a.counters && Q.q == 0)
 #pragma unroll
@@ -1130,7 +1138,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             norm = r * r;
         }
         norm = Q.sum(norm);
-        const bool miss = !(norm < ctl.outer_tolerance * ctl.outer_tolerance);
+        const bool miss = capped || !(norm < ctl.outer_tolerance * ctl.outer_tolerance);
         if (Q.q == 0) {
             int32_t* stp = status();
             if (skipped) {

@@ -277,11 +277,18 @@ SolverControls controls(const unblending_solver_options& so) {
 
 // Controls of the FP32 solve. When its misses are re-solved in FP64, the FP32
 // solve stops after fp32_outer outer steps: a pixel still unsolved by then
-// almost never converges later (it runs to the outer cap and fails), and the
-// FP64 re-solve gives it the reference method's own result anyway.
+// mostly never converges (92% of those run to the outer cap and fail, at
+// ~1050 evaluations each against ~100 for a converging pixel), and every
+// pixel stopped unconverged, whatever its best point, goes to the FP64
+// re-solve, which gives it the reference method's own result. Measured on
+// 1024x1024, 5 layers (ms of FP32 solve + FP64 re-solve, both passes): cap 9
+// 183.7, 10 184.2, 11 187.4, 12 192.1.
 SolverControls fp32_controls(const unblending_solver_options& so) {
     SolverControls c = controls(so);
-    if (so.resolve_misses && so.fp32_outer > 0 && so.fp32_outer < c.outer) c.outer = so.fp32_outer;
+    if (so.resolve_misses && so.fp32_outer > 0 && so.fp32_outer < c.outer) {
+        c.outer = so.fp32_outer;
+        c.cap_is_miss = 1;
+    }
     return c;
 }
 
