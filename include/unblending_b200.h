@@ -207,6 +207,23 @@ UNBLENDING_API int32_t unblending_unmix_batch_device(
 /* Number of GPU kernel launches the most recent call on this thread issued. */
 UNBLENDING_API int64_t unblending_last_launch_count(void);
 
+/* LayerInfos JSON, the reference's layer-info file (LayerInfos.md;
+ * unblending/src/unblending_io.cpp:141-170 import_layer_infos). Host only.
+ * Parses NUL-terminated `json` into at most `capacity` layers, bottom first,
+ * with the precision = inverse of the file's covariance; *count receives the
+ * file's layer count (UNBLENDING_BUFFER_TOO_SMALL when it exceeds capacity).
+ * Malformed text, an unknown mode name or a singular covariance:
+ * UNBLENDING_INVALID_ARGUMENT. */
+UNBLENDING_API int32_t unblending_parse_layer_infos(const char* json, unblending_layer* layers, size_t capacity,
+                                                    size_t* count);
+
+/* JSON text of `layer_count` layers in the same format
+ * (unblending_io.cpp:125-139 export_layer_infos): writes it NUL-terminated to
+ * `text` when `capacity` bytes suffice; *length receives its length without
+ * the NUL (UNBLENDING_BUFFER_TOO_SMALL when it does not fit). */
+UNBLENDING_API int32_t unblending_format_layer_infos(const unblending_layer* layers, size_t layer_count, char* text,
+                                                     size_t capacity, size_t* length);
+
 #ifdef __cplusplus
 }
 #endif

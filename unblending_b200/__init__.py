@@ -166,6 +166,12 @@ def _load():
     lib.unblending_unmix_device_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]
+    lib.unblending_parse_layer_infos.restype = ctypes.c_int32
+    lib.unblending_parse_layer_infos.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t,
+                                                 P(ctypes.c_size_t)]
+    lib.unblending_format_layer_infos.restype = ctypes.c_int32
+    lib.unblending_format_layer_infos.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_char_p,
+                                                  ctypes.c_size_t, P(ctypes.c_size_t)]
     return lib
 
 

@@ -36,6 +36,7 @@ UNITS = [
     ("mlp.cu", []),
     ("mlp_data.cu", []),
     ("pixels.cpp", ["-I" + os.path.join(ROOT, "include")]),
+    ("layer_infos.cpp", ["-I" + os.path.join(ROOT, "include")]),
     ("unblending_c.cpp", []),
 ]
 

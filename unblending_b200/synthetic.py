@@ -54,9 +54,14 @@ class LayerSpec:
     mean: np.ndarray
     covariance: np.ndarray
     comp: tuple = SOURCE_OVER
+    # Precision given as is (a layer-info file's), instead of one derived
+    # from the covariance.
+    precision_matrix: np.ndarray | None = None
 
     @property
     def precision(self) -> np.ndarray:
+        if self.precision_matrix is not None:
+            return np.asarray(self.precision_matrix, dtype=np.float64).reshape(3, 3)
         p = np.linalg.inv(self.covariance)
         return 0.5 * (p + p.T)
 
