@@ -58,10 +58,14 @@ typedef struct unblending_solver_options {
                                    at least gradient_quorum/8 of the warp's pixels need one (or none needs a
                                    value alone); the others wait one evaluation. 0 = never wait. Results do not
                                    depend on it. Default 3, range 0..8 */
+    int32_t resolve_frozen_stop;/* FP32 precision with resolve_misses: the FP64 re-solve stops a pixel after this
+                                   many consecutive outer steps that moved neither its point nor its best point
+                                   (default 4; 0 = run to the outer cap, the reference's schedule). The FP64
+                                   precision solve always runs to the cap */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 9, 3 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 9, 3, 4 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

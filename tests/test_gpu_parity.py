@@ -279,3 +279,32 @@ def test_warp_scheduling_quorum_leaves_results_unchanged(cuda, precision):
     for other in outs[1:]:
         for a, b in zip(outs[0], other):
             assert np.array_equal(a, b)
+
+
+FROZEN_CASES = [
+    ("rgb1024_l5", 160, 128, None),
+    ("rgb4096_l6", 160, 128, None),
+]
+
+
+@pytest.mark.parametrize("case", range(len(FROZEN_CASES) + 2))
+def test_resolve_frozen_stop_leaves_results_unchanged(cuda, case):
+    """The FP64 re-solve stops a pixel after 4 outer steps that moved neither
+    its point nor its best point; the outputs equal those of the full
+    schedule (frozen stop off) on these images, both passes."""
+    if case < len(FROZEN_CASES):
+        name, w, h, _ = FROZEN_CASES[case]
+        wl = syn.workload(name, w, h)
+    elif case == len(FROZEN_CASES):
+        wl = syn.generate(128, 96, [0, 6, 7, 9, 1], (8.0, 40.0), seed=8)
+    else:
+        wl = syn.batch(count=2, seed=21, sides=(256, 320))[0]
+    outs = []
+    for stop in (0, 4):
+        so = solver(cuda, 0, radius=4, resolve_frozen_stop=stop)
+        first, st1, _, s1 = cuda.unmix_ex(wl.image, wl.layers, solver=so)
+        final, st2, _, s2 = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so)
+        outs.append((first, st1, final, st2))
+    print("frozen stop case", case, "misses", s1["misses"], s2["misses"])
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)

@@ -64,6 +64,7 @@ struct SolverControls {
     int gradient_quorum = 3;           // eighths of a warp's live pixels that start a gradient evaluation
     int direction_quorum = 0;          // eighths of a warp's live pixels that start a new direction (0 = no wait)
     int cap_is_miss = 0;               // a pixel that reaches the outer cap unconverged is a miss
+    int frozen_stop = 0;               // stop after this many outer steps that move neither x nor the best point
 };
 
 // One image of a batched first pass: its pixels occupy global queue indices

@@ -299,6 +299,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 
     // Per-quad scalars (uniform within the quad).
     int phase, start, outer, it, attempt, bt, valid;
+    int frozen;      // consecutive outer steps that moved neither x nor the best point
+    bool best_moved; // the best point changed during this outer step
     T rho, f, oldnorm, step, slope, cand;
     T best_norm, best_energy;
     bool have_best;
@@ -464,6 +466,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
                  (!feasible && best_norm >= tol2 && norm < best_norm))) {
                 have_best = true; best_norm = norm; best_energy = energy;
+                best_moved = true;
 #pragma unroll
                 for (int l = 0; l < L; ++l) best(l) = tr[l];
             }
@@ -879,6 +882,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         for (int r = 0; r < R; ++r) lam[r] = T(0);
         rho = T(100);
         outer = 0;
+        frozen = 0;
         return aBeginOuter;
     }
 
@@ -887,6 +891,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 #pragma unroll
         for (int l = 0; l < L; ++l) { ox(l) = X(l); tr[l] = X(l); }
         phase = kOuterEval;
+        best_moved = false;
         return aEval;
     }
 
@@ -910,6 +915,15 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 #pragma unroll
         for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion = madd(dl, dl, motion); }
         motion = Q.sum(motion);
+        // A pixel whose last frozen_stop outer steps moved neither x nor the
+        // best point stops here: past that point the method has not been
+        // seen to change its result (its outputs equal the full run's on
+        // every tested image); with frozen_stop = 0 it runs to the cap.
+        frozen = (motion == T(0) && !best_moved) ? frozen + 1 : 0;
+        if (ctl.frozen_stop > 0 && frozen >= ctl.frozen_stop) {
+            if (start + 1 < ctl.starts) { ++start; return aBeginStart; }
+            return aFinish;
+        }
         if (!(motion < tol2 && feasible)) {
             if (outer + 1 < ctl.outer) {
                 ++outer;
