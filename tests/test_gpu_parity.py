@@ -287,23 +287,30 @@ FROZEN_CASES = [
 ]
 
 
-@pytest.mark.parametrize("case", range(len(FROZEN_CASES) + 2))
+@pytest.mark.parametrize("case", range(len(FROZEN_CASES) + 4))
 def test_resolve_frozen_stop_leaves_results_unchanged(cuda, case):
     """The FP64 re-solve stops a pixel after 4 outer steps that moved neither
     its point nor its best point; the outputs equal those of the full
-    schedule (frozen stop off) on these images, both passes."""
+    schedule (frozen stop off) on these images, both passes (three starts
+    and a non-opaque Plus stack included)."""
+    opaque, smooth, starts = True, True, 1
     if case < len(FROZEN_CASES):
         name, w, h, _ = FROZEN_CASES[case]
         wl = syn.workload(name, w, h)
     elif case == len(FROZEN_CASES):
         wl = syn.generate(128, 96, [0, 6, 7, 9, 1], (8.0, 40.0), seed=8)
-    else:
+    elif case == len(FROZEN_CASES) + 1:
         wl = syn.batch(count=2, seed=21, sides=(256, 320))[0]
+    elif case == len(FROZEN_CASES) + 2:
+        wl, starts = syn.workload("rgb1024_l5", 96, 80), 3
+    else:
+        wl = syn.generate(96, 80, [0, 1, 2], (4.0, 12.0), seed=7, comp=syn.PLUS)
+        opaque, smooth = False, False
     outs = []
     for stop in (0, 4):
-        so = solver(cuda, 0, radius=4, resolve_frozen_stop=stop)
-        first, st1, _, s1 = cuda.unmix_ex(wl.image, wl.layers, solver=so)
-        final, st2, _, s2 = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so)
+        so = solver(cuda, 0, radius=4, resolve_frozen_stop=stop, starts=starts)
+        first, st1, _, s1 = cuda.unmix_ex(wl.image, wl.layers, opaque=opaque, solver=so)
+        final, st2, _, s2 = cuda.refine_ex(wl.image, first, wl.layers, opaque=opaque, smooth=smooth, solver=so)
         outs.append((first, st1, final, st2))
     print("frozen stop case", case, "misses", s1["misses"], s2["misses"])
     for a, b in zip(*outs):
