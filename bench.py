@@ -328,8 +328,8 @@ class Decomposition:
 
 def train_warm_start(U, torch, wl):
     """The warm-start network for this layer set: 64 seeded 256x256 images of
-    the workload's distributions (2^22 pixels), batch 8192, 512 Adam steps at
-    lr 1e-3."""
+    the workload's distributions (2^22 pixels), batch 8192, 2048 Adam steps
+    (four passes over the pixels) at lr 1e-3."""
     from unblending_b200 import synthetic as syn
     modes = [s.mode for s in wl.layers]
     t0 = time.perf_counter()
@@ -338,10 +338,10 @@ def train_warm_start(U, torch, wl):
     d = [torch.from_numpy(w.image.reshape(-1)).cuda() for w in imgs]
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
-    model = U.mlp_train_device([(x.data_ptr(), 256, 256) for x in d], wl.layers, batch=8192, steps=512,
+    model = U.mlp_train_device([(x.data_ptr(), 256, 256) for x in d], wl.layers, batch=8192, steps=2048,
                                learning_rate=1e-3, seed=1)
     torch.cuda.synchronize()
-    return model, {"images": 64, "pixels": 64 * 256 * 256, "batch": 8192, "steps": 512, "lr": 1e-3,
+    return model, {"images": 64, "pixels": 64 * 256 * 256, "batch": 8192, "steps": 2048, "lr": 1e-3,
                    "final_batch_mse": model.loss, "train_s": time.perf_counter() - t0, "generate_s": t_gen}
 
 
