@@ -1218,17 +1218,20 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             // recomputes the residuals of that point unchanged.
             bool allow_bi = bq == 0;
             for (;;) {
+                // The actions in the order the method chains them, each at
+                // most once per pass: pixels that reach an action from
+                // different points of their chains (a line-search step, or an
+                // accept followed by a new direction) run it together. A
+                // pixel's own sequence of actions is unchanged.
                 while (act != aEval && (allow_bi || act != aBeginIter)) {
-                    switch (act) {
-                    case aBeginIter: act = begin_iteration(); break;
-                    case aNextTrial: act = next_trial(); break;
-                    case aAccept: act = accept(); break;
-                    case aEndOuter: act = end_outer(); break;
-                    case aBeginStart: act = begin_start(); break;
-                    case aBeginOuter: act = begin_outer(); break;
-                    case aFinish: store(false); act = aFetch; break;
-                    default: act = fetch(total, live); break;
-                    }
+                    if (act == aAccept) act = accept();
+                    if (act == aBeginIter && allow_bi) act = begin_iteration();
+                    if (act == aNextTrial) act = next_trial();
+                    if (act == aEndOuter) act = end_outer();
+                    if (act == aFinish) { store(false); act = aFetch; }
+                    if (act == aFetch) act = fetch(total, live);
+                    if (act == aBeginStart) act = begin_start();
+                    if (act == aBeginOuter) act = begin_outer();
                 }
                 if (allow_bi) break;
                 const int nb = __popc(__ballot_sync(0xffffffffu, act == aBeginIter));
