@@ -229,6 +229,26 @@ def cpu_reference(wl, first_gpu, finals, threads, sample_idx):
         parity[name] = {"first_pass": report(g1, ref1, wl.layers, False),
                         "refinement_same_first_pass": report(g2, ref2, wl.layers, True) if name == "plain" else None}
     details = {"t_unmix_sample_s": t_unmix, "t_refine_sample_s": t_refine, "t_filter_full_s": t_filter}
+    # The same on one host core: both solves over the first 512 sample pixels,
+    # the filter over the whole image.
+    k = min(512, m)
+    t0 = time.perf_counter()
+    impl.solve(layers, oracle.problem(L, False, True), oracle.options(), target[:k], init[:k], threads=1)
+    t1_unmix = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    if kind == "reference":
+        impl.dll.ref_refine_targets(rgb_planar.ctypes.data_as(oracle._dp), first_planar.ctypes.data_as(oracle._dp),
+                                    layers, L, w, h, 1, 1, radius, 1, targets.ctypes.data_as(oracle._dp),
+                                    status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        t1_filter = time.perf_counter() - t0
+    else:
+        t1_filter = t_filter
+    t0 = time.perf_counter()
+    impl.solve(layers, oracle.problem(L, True, True, True), oracle.options(), target[:k], init2[:k], alpha=alpha[:k],
+               bg=bg[:k], threads=1)
+    t1_refine = time.perf_counter() - t0
+    details["single_core"] = {"value": n / (t1_filter + (t1_unmix + t1_refine) / k * n), "cores": 1,
+                              "sample": f"both solves on {k} sample pixels, the filter over the full image"}
     return seconds, kind, details, parity
 
 
