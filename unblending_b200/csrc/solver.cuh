@@ -1246,12 +1246,13 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                                              (phase == kTrial && bt == 0 && ctl.gradient_on_first_trial));
             // The warp runs the gradient part of an evaluation if any of its
             // pixels needs it, with the others masked off. While fewer than
-            // gradient_quorum/8 of the live pixels need a gradient (and some
-            // need a value alone), those pixels wait: this evaluation is
-            // value-only, and they evaluate with the next quorum. A waiting
-            // pixel's evaluate() is inactive and recomputes the residuals of
-            // its unchanged trial point, which its own evaluation then
-            // recomputes identically, so its results do not change.
+            // gradient_quorum/8 of the pixels ready to evaluate need a
+            // gradient (and some need a value alone), those pixels wait: this
+            // evaluation is value-only, and they evaluate with the next
+            // quorum. A waiting pixel's evaluate() is inactive and recomputes
+            // the residuals of its unchanged trial point, which its own
+            // evaluation then recomputes identically, so its results do not
+            // change.
             bool go = ready;
             if (gq > 0) {
                 const int ng = __popc(__ballot_sync(0xffffffffu, need_grad));
