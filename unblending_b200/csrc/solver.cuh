@@ -1003,7 +1003,16 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             sv[l] = tr[l] - X(l);
             yv[l] = ng[l] - G(l);
             sy = madd(sv[l], yv[l], sy); ss = madd(sv[l], sv[l], ss); yy = madd(yv[l], yv[l], yy);
-            mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
+            if constexpr (kFast || !Slice::kRolledEval) mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
+        }
+        if constexpr (!kFast && Slice::kRolledEval) {
+            // One copy of the FP64 division: the step from the accepted point
+            // (the last point evaluated, kept in the scratch slice) per layer.
+#pragma unroll 1
+            for (int l = 0; l < L; ++l) {
+                const T x = X(l), s = Slice::value(Slice::kScratch + l) - x;
+                mm = fmax(mm, qdiv(fabs(s), T(1) + fabs(x)));
+            }
         }
         Q.sum3(sy, ss, yy);
         if constexpr (kLanes == 3) {
