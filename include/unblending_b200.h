@@ -157,6 +157,24 @@ UNBLENDING_API int32_t unblending_refine_device(
     const double* first_pass, const unblending_options* options, const unblending_solver_options* solver,
     double* output, int32_t* status, uint32_t* counters, void* stream, unblending_stats* stats);
 
+/* The same two passes restricted to the pixels of rows [row_begin, row_end)
+ * of the image (0 <= row_begin <= row_end <= height): only their outputs,
+ * status and counters are written. The refinement's guided filter still
+ * covers the whole image and reads the whole first pass, so a band's results
+ * equal the whole-image call's for its rows bit for bit: an image split into
+ * row bands (one per GPU) and the first pass gathered between the passes
+ * decomposes exactly as on one GPU. */
+UNBLENDING_API int32_t unblending_unmix_device_rows(
+    int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
+    const unblending_options* options, const unblending_solver_options* solver, double* output, int32_t* status,
+    uint32_t* counters, int32_t row_begin, int32_t row_end, void* stream, unblending_stats* stats);
+
+UNBLENDING_API int32_t unblending_refine_device_rows(
+    int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
+    const double* first_pass, const unblending_options* options, const unblending_solver_options* solver,
+    double* output, int32_t* status, uint32_t* counters, int32_t row_begin, int32_t row_end, void* stream,
+    unblending_stats* stats);
+
 /* First pass that allocates nothing. No counterpart in the reference: it
  * exists for callers that must not allocate device memory inside their
  * processing call, such as a host application that owns all device memory

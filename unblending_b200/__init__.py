@@ -150,6 +150,16 @@ def _load():
                                              ctypes.c_size_t, ctypes.c_void_p, P(Options), P(SolverOptions),
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              P(Stats)]
+    lib.unblending_unmix_device_rows.restype = ctypes.c_int32
+    lib.unblending_unmix_device_rows.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_size_t, P(Options), P(SolverOptions), ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.c_void_p, P(Stats)]
+    lib.unblending_refine_device_rows.restype = ctypes.c_int32
+    lib.unblending_refine_device_rows.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_size_t, ctypes.c_void_p, P(Options), P(SolverOptions),
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                                  ctypes.c_int32, ctypes.c_void_p, P(Stats)]
     lib.unblending_last_launch_count.restype = ctypes.c_int64
     lib.unblending_mlp_train_device.restype = ctypes.c_int32
     lib.unblending_mlp_train_device.argtypes = [ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32),
@@ -296,6 +306,32 @@ def refine_device(width, height, d_image, layers, d_first, d_output, opaque=True
     rc = lib.unblending_refine_device(width, height, d_image, arr, L, d_first, ctypes.byref(options(opaque, smooth)),
                                       ctypes.byref(solver or solver_options()), d_output, d_status, d_counters, stream,
                                       ctypes.byref(st) if stats else None)
+    _check(rc)
+    return st.as_dict() if stats else None
+
+
+def unmix_device_rows(width, height, d_image, layers, d_output, row_begin, row_end, opaque=True, solver=None,
+                      d_status=None, d_counters=None, stream=None, stats=False):
+    """unmix_device restricted to rows [row_begin, row_end) of the image."""
+    arr, L = _layers(layers)
+    st = Stats(); st.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_unmix_device_rows(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+                                          ctypes.byref(solver or solver_options()), d_output, d_status, d_counters,
+                                          row_begin, row_end, stream, ctypes.byref(st) if stats else None)
+    _check(rc)
+    return st.as_dict() if stats else None
+
+
+def refine_device_rows(width, height, d_image, layers, d_first, d_output, row_begin, row_end, opaque=True,
+                       smooth=False, solver=None, d_status=None, d_counters=None, stream=None, stats=False):
+    """refine_device restricted to rows [row_begin, row_end); the filter covers
+    the whole image (d_first must hold the whole first pass)."""
+    arr, L = _layers(layers)
+    st = Stats(); st.struct_size = ctypes.sizeof(Stats)
+    rc = lib.unblending_refine_device_rows(width, height, d_image, arr, L, d_first,
+                                           ctypes.byref(options(opaque, smooth)),
+                                           ctypes.byref(solver or solver_options()), d_output, d_status, d_counters,
+                                           row_begin, row_end, stream, ctypes.byref(st) if stats else None)
     _check(rc)
     return st.as_dict() if stats else None
 

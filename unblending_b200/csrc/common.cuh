@@ -112,6 +112,9 @@ struct SolveArgs {
     // history_lanes lanes; the launch uses at most history_lanes / 128 blocks.
     void* history = nullptr;
     int history_lanes = 0;
+    // Without a list: the launch solves pixels [first_pixel, first_pixel +
+    // pixel_count) of the image (pixel_count < 0: all n).
+    int first_pixel = 0, pixel_count = -1;
 };
 
 }  // namespace unb

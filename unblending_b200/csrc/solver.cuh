@@ -1182,7 +1182,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
         job = Q.from(job, 0);
         if (job >= total) { phase = kIdle; live = false; return aEval; }
-        gidx = a.list ? a.list[job] : job;
+        gidx = a.list ? a.list[job] : a.first_pixel + job;
         int i = gidx;
         if constexpr (BATCH) {
             // The image owning queue index gidx: last job with offset <= gidx.
@@ -1214,7 +1214,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 
     // ------------------------------------------------------------- loop --
     __device__ void run() {
-        const int total = a.list ? *a.list_count : a.n;
+        const int total = a.list ? *a.list_count : (a.pixel_count >= 0 ? a.pixel_count : a.n);
         bool live = !Q.extra;            // lanes of no group stay idle throughout
         int act = live ? aFetch : aEval;
         const int gq = ctl.gradient_quorum, bq = ctl.direction_quorum;

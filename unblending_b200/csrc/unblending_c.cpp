@@ -377,6 +377,7 @@ struct PassIO {
     double* out = nullptr;           // device
     int32_t* status = nullptr;       // device, per pixel (context buffer when the caller passes none)
     uint32_t* counters = nullptr;    // device or null
+    int first_pixel = 0, pixel_count = -1;   // the pixels solved (rows of the image); -1: all
 };
 
 struct PassResult {
@@ -416,6 +417,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     const SolverControls ctl = controls(so), ctl32 = fp32_controls(so), ctl_re = resolve_controls(so);
     SolveArgs a;
     a.n = int(n);
+    a.first_pixel = io.first_pixel; a.pixel_count = io.pixel_count;
     a.image = io.image; a.first = io.first; a.targets = targets; a.out = io.out;
     a.status = io.status; a.counters = io.counters;
     a.input_status = fstatus; a.input_failed = counts + 2;
@@ -577,12 +579,15 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
 int32_t device_call(int32_t width, int32_t height, const double* image, const unblending_layer* layers,
                     size_t layer_count, const double* first, const unblending_options* options,
                     const unblending_solver_options* solver, double* output, int32_t* status, uint32_t* counters,
-                    void* stream, unblending_stats* stats, bool refine) {
+                    void* stream, unblending_stats* stats, bool refine, int32_t row_begin = 0,
+                    int32_t row_end = -1) {
     t_launches = 0;
     unblending_rgb_view view{image, 0, width, height, 0};
     Spec sp;
     int32_t rc = validate(&view, layers, layer_count, options, output, 0, refine, first, 0, sp, true);
     if (rc != UNBLENDING_OK) return rc;
+    if (row_end < 0) row_end = height;
+    if (row_begin < 0 || row_begin > row_end || row_end > height) return UNBLENDING_INVALID_ARGUMENT;
     unblending_solver_options so;
     if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
     if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
@@ -604,13 +609,15 @@ int32_t device_call(int32_t width, int32_t height, const double* image, const un
         }
         io.status = status ? status : c.status.get<int32_t>(sp.pixels);
         io.counters = counters;
+        io.first_pixel = row_begin * width;
+        io.pixel_count = (row_end - row_begin) * width;
         PassResult R = enqueue_pass(c, sp, refine, layers, so, io, s);
         if (stats) {
             int32_t counts[3] = {0, 0, 0};
             ck(cudaMemcpyAsync(counts, R.small, sizeof(counts), cudaMemcpyDeviceToHost, s));
             ck(cudaStreamSynchronize(s));
             stats->radius = R.radius;
-            stats->pixels = int64_t(sp.pixels);
+            stats->pixels = int64_t(row_end - row_begin) * width;
             stats->misses = counts[0];
             stats->failed = counts[1];
             stats->normalization_failed = counts[2];
@@ -676,6 +683,24 @@ int32_t unblending_refine_device(int32_t width, int32_t height, const double* im
                                  uint32_t* counters, void* stream, unblending_stats* stats) {
     return device_call(width, height, image, layers, layer_count, first_pass, options, solver, output, status,
                        counters, stream, stats, true);
+}
+
+int32_t unblending_unmix_device_rows(int32_t width, int32_t height, const double* image,
+                                     const unblending_layer* layers, size_t layer_count,
+                                     const unblending_options* options, const unblending_solver_options* solver,
+                                     double* output, int32_t* status, uint32_t* counters, int32_t row_begin,
+                                     int32_t row_end, void* stream, unblending_stats* stats) {
+    return device_call(width, height, image, layers, layer_count, nullptr, options, solver, output, status, counters,
+                       stream, stats, false, row_begin, row_end);
+}
+
+int32_t unblending_refine_device_rows(int32_t width, int32_t height, const double* image,
+                                      const unblending_layer* layers, size_t layer_count, const double* first_pass,
+                                      const unblending_options* options, const unblending_solver_options* solver,
+                                      double* output, int32_t* status, uint32_t* counters, int32_t row_begin,
+                                      int32_t row_end, void* stream, unblending_stats* stats) {
+    return device_call(width, height, image, layers, layer_count, first_pass, options, solver, output, status,
+                       counters, stream, stats, true, row_begin, row_end);
 }
 
 int64_t unblending_last_launch_count(void) { return t_launches; }
