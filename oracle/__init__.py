@@ -36,11 +36,13 @@ class Problem(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("history", ctypes.c_int32), ("inner", ctypes.c_int32), ("outer", ctypes.c_int32),
                 ("starts", ctypes.c_int32), ("canonical", ctypes.c_int32),
-                ("inner_tolerance", ctypes.c_double), ("outer_tolerance", ctypes.c_double)]
+                ("inner_tolerance", ctypes.c_double), ("outer_tolerance", ctypes.c_double),
+                ("frozen_stop", ctypes.c_int32)]
 
 
-def options(history=6, inner=256, outer=22, starts=1, canonical=False, inner_tolerance=5e-3, outer_tolerance=5e-3):
-    return Options(history, inner, outer, starts, int(canonical), inner_tolerance, outer_tolerance)
+def options(history=6, inner=256, outer=22, starts=1, canonical=False, inner_tolerance=5e-3, outer_tolerance=5e-3,
+            frozen_stop=0):
+    return Options(history, inner, outer, starts, int(canonical), inner_tolerance, outer_tolerance, frozen_stop)
 
 
 def problem(layers, refinement=False, opaque=True, smooth=False):

@@ -25,6 +25,7 @@ typedef struct orc_layer {
 typedef struct orc_options {
     int32_t history, inner, outer, starts, canonical;
     double inner_tolerance, outer_tolerance;
+    int32_t frozen_stop;
 } orc_options;
 
 typedef struct orc_problem {
@@ -59,6 +60,7 @@ Options to_options(const orc_options* o) {
         opt.history = o->history; opt.inner = o->inner; opt.outer = o->outer; opt.starts = o->starts;
         opt.canonical = o->canonical != 0;
         opt.inner_tolerance = o->inner_tolerance; opt.outer_tolerance = o->outer_tolerance;
+        opt.frozen_stop = o->frozen_stop;
     }
     return opt;
 }

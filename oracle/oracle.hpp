@@ -70,6 +70,11 @@ struct Options {
     int history = 6, inner = 256, outer = 22, starts = 1;
     bool canonical = false;
     double inner_tolerance = 5e-3, outer_tolerance = 5e-3;
+    // Not in the reference: stop a start after this many consecutive outer
+    // steps that moved neither x nor the best point (0 = never), the rule the
+    // CUDA path's FP64 re-solve applies; lets the tests check on the CPU that
+    // it leaves the results unchanged.
+    int frozen_stop = 0;
 };
 
 struct Counters {
@@ -302,6 +307,7 @@ template <class T> struct Solver {
     T hs[kMaxHistory][kMaxN], hy[kMaxHistory][kMaxN], coeff[kMaxHistory], inv[kMaxHistory];
     T best_norm, best_energy;
     bool have_best;
+    long best_updates = 0;
 
     T lo(int k) const { return bound(p, alpha, bg, k, false); }
     T hi(int k) const { return bound(p, alpha, bg, k, true); }
@@ -321,6 +327,7 @@ template <class T> struct Solver {
              (!feasible && best_norm >= tol && norm < best_norm))) {
             have_best = true; best_norm = norm; best_energy = energy;
             for (int k = 0; k < N; ++k) best[k] = point[k];
+            ++best_updates;
         }
         return value;
     }
@@ -490,8 +497,10 @@ template <class T> struct Solver {
     void augmented_lagrangian(T rho) {
         const T tol2 = T(opt.outer_tolerance * opt.outer_tolerance);
         {
+            int frozen = 0;
             for (int outer = 0; outer < opt.outer; ++outer) {
                 if (counters) ++counters->outer;
+                const long updates_before = best_updates;
                 if (opt.canonical) canonicalize(x);
                 for (int k = 0; k < N; ++k) outer_x[k] = x[k];
                 T f = eval(x, g, rho, true);
@@ -567,6 +576,8 @@ template <class T> struct Solver {
                 for (int r = 0; r < C; ++r) lambda[r] -= rho * residual[r];
                 if (norm > T(0.0625) * oldnorm) rho *= T(10);
                 for (int k = 0; k < N; ++k) { const T d = x[k] - outer_x[k]; motion += d * d; }
+                frozen = (motion == T(0) && best_updates == updates_before) ? frozen + 1 : 0;
+                if (opt.frozen_stop > 0 && frozen >= opt.frozen_stop) break;
                 if (motion < tol2 && feasible) break;
             }
         }
