@@ -58,10 +58,10 @@ typedef struct unblending_solver_options {
                                    at least gradient_quorum/8 of the warp's pixels need one (or none needs a
                                    value alone); the others wait one evaluation. 0 = never wait. Results do not
                                    depend on it. Default 3, range 0..8 */
-    int32_t resolve_frozen_stop;/* FP32 precision with resolve_misses: the FP64 re-solve stops a pixel after this
-                                   many consecutive outer steps that moved neither its point nor its best point
-                                   (default 4; 0 = run to the outer cap, the reference's schedule). The FP64
-                                   precision solve always runs to the cap */
+    int32_t frozen_stop;        /* FP64 solves (the FP64 precision solve, and the re-solve behind the FP32 solve)
+                                   stop a pixel after this many consecutive outer steps that moved neither its
+                                   point nor its best point (default 4; 0 = run to the outer cap, the
+                                   reference's schedule; results equal on every tested image) */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \

@@ -288,7 +288,7 @@ FROZEN_CASES = [
 
 
 @pytest.mark.parametrize("case", range(len(FROZEN_CASES) + 4))
-def test_resolve_frozen_stop_leaves_results_unchanged(cuda, case):
+def test_frozen_stop_leaves_results_unchanged(cuda, case):
     """The FP64 re-solve stops a pixel after 4 outer steps that moved neither
     its point nor its best point; the outputs equal those of the full
     schedule (frozen stop off) on these images, both passes (three starts
@@ -308,7 +308,7 @@ def test_resolve_frozen_stop_leaves_results_unchanged(cuda, case):
         opaque, smooth = False, False
     outs = []
     for stop in (0, 4):
-        so = solver(cuda, 0, radius=4, resolve_frozen_stop=stop, starts=starts)
+        so = solver(cuda, 0, radius=4, frozen_stop=stop, starts=starts)
         first, st1, _, s1 = cuda.unmix_ex(wl.image, wl.layers, opaque=opaque, solver=so)
         final, st2, _, s2 = cuda.refine_ex(wl.image, first, wl.layers, opaque=opaque, smooth=smooth, solver=so)
         outs.append((first, st1, final, st2))

@@ -219,7 +219,7 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
                                         out.threads_per_block > 128)) ||
         out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
         out.fp64_variant >= kFp64Variants || out.fp32_outer < 0 || out.gradient_quorum < 0 ||
-        out.gradient_quorum > 8 || out.resolve_frozen_stop < 0)
+        out.gradient_quorum > 8 || out.frozen_stop < 0)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -272,6 +272,23 @@ SolverControls controls(const unblending_solver_options& so) {
     // refinement) but not in the FP32 solve (50 -> 52 ms) or in the FP64
     // re-solve of the FP32 misses (44 -> 45 ms).
     c.direction_quorum = so.precision == UNBLENDING_PRECISION_FP64 ? 3 : 0;
+    // FP64 solves stop a pixel once frozen_stop consecutive outer steps moved
+    // neither its point nor its best point. Oracle traces of every pixel of
+    // eleven images (1024x1024 five-layer, 4096-size six-layer crop, six of
+    // the uneven batch, dodge/burn/soft-light stacks; both passes): with 4 such
+    // steps no pixel's best point moved afterwards, so the outputs equal the
+    // full schedule's, while 11-39 % of the outer steps were left out (all of
+    // them steps of pixels that end unsolved, at ~66 evaluations a step). The
+    // FP32 solve never freezes that way before its cap.
+    c.frozen_stop = so.precision == UNBLENDING_PRECISION_FP64 ? so.frozen_stop : 0;
+    return c;
+}
+
+// Controls of the FP64 re-solve behind the FP32 solve: the method's own, with
+// the frozen stop (controls() sets it for the FP64 precision solve too).
+SolverControls resolve_controls(const unblending_solver_options& so) {
+    SolverControls c = controls(so);
+    c.frozen_stop = so.frozen_stop;
     return c;
 }
 
@@ -283,20 +300,6 @@ SolverControls controls(const unblending_solver_options& so) {
 // re-solve, which gives it the reference method's own result. Measured on
 // 1024x1024, 5 layers (ms of FP32 solve + FP64 re-solve, both passes): cap 9
 // 183.7, 10 184.2, 11 187.4, 12 192.1.
-// Controls of the FP64 re-solve behind the FP32 solve: the method's own, and
-// a pixel stops once resolve_frozen_stop consecutive outer steps moved
-// neither its point nor its best point. Oracle traces of every pixel of eleven
-// images (1024x1024 five-layer, 4096-size six-layer crop, six of the uneven
-// batch, dodge/burn/soft-light stacks; both passes): with 4 such steps no
-// pixel's best point moved afterwards, so the outputs equal the full
-// schedule's, while 11-39 % of the outer steps were left out (all of them
-// steps of pixels that end unsolved, at ~66 evaluations a step).
-SolverControls resolve_controls(const unblending_solver_options& so) {
-    SolverControls c = controls(so);
-    c.frozen_stop = so.resolve_frozen_stop;
-    return c;
-}
-
 SolverControls fp32_controls(const unblending_solver_options& so) {
     SolverControls c = controls(so);
     if (so.resolve_misses && so.fp32_outer > 0 && so.fp32_outer < c.outer) {
@@ -742,7 +745,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
     put(&so, offsetof(unblending_solver_options, warm_start));
     put(&so.fp64_variant, sizeof(so.fp64_variant)); put(&so.fp32_outer, sizeof(so.fp32_outer));
     put(&so.gradient_quorum, sizeof(so.gradient_quorum));
-    put(&so.resolve_frozen_stop, sizeof(so.resolve_frozen_stop));
+    put(&so.frozen_stop, sizeof(so.frozen_stop));
     for (int k = 0; k < count; ++k) {
         const auto& J = jobs[k];
         put(&J.width, sizeof(J.width)); put(&J.height, sizeof(J.height));
