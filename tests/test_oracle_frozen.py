@@ -32,3 +32,14 @@ def test_frozen_stop_leaves_oracle_results_unchanged(case):
     assert np.array_equal(a1, b1), name
     assert np.array_equal(a2, b2), name
     assert outer_steps[1] < outer_steps[0], (name, outer_steps)
+
+
+def test_frozen_stop_with_three_starts():
+    """With three starts a frozen start ends and the next one begins, as at
+    the outer cap; results equal the full schedule's."""
+    wl = syn.workload("rgb1024_l5", 96, 64)
+    outs = []
+    for stop in (0, 4):
+        x, _ = oracle.unmix(wl.image, wl.layers, opts=oracle.options(starts=3, frozen_stop=stop))
+        outs.append(x)
+    assert np.array_equal(outs[0], outs[1])
