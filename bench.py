@@ -14,7 +14,8 @@ reference's refinement radius 60*min(w,h)/1000 = 61.
                trained beforehand on 64 seeded 256x256 images of the same layer
                set, 2^22 pixels, batch 8192, Adam lr 1e-3).
   fp64       : the same with the FP64 solve (replays the reference's FP64
-               solver).
+               solver; pixels whose outer steps stop moving them end early,
+               with results equal to the full schedule).
   e2e        : the plain configuration through the C ABI calls
                unblending_unmix + unblending_refine with pinned host buffers.
 
