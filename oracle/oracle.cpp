@@ -258,6 +258,37 @@ int orc_solve(const orc_layer* layers, const orc_problem* problem, const orc_opt
     return 0;
 }
 
+// The same method in FP32 arithmetic (the oracle templated on float; inputs
+// rounded to float, results widened back): how far a change of precision
+// alone moves the method's results.
+int orc_solve_f32(const orc_layer* layers, const orc_problem* problem, const orc_options* options, size_t n,
+                  const double* target, const double* alpha, const double* bg, const double* initial, double* out,
+                  int threads) {
+    if (!problem || problem->layers <= 0 || problem->layers > kMaxLayers) return 1;
+    const auto models = to_layers(layers, problem->layers);
+    const Problem p = to_problem(problem);
+    const Options opt = to_options(options);
+    if (opt.history <= 0 || opt.history > kMaxHistory) return 1;
+    const int L = p.layers, N = 4 * L;
+    parallel_for(n, threads, [&](size_t b, size_t e) {
+        Solver<float> s;
+        s.models = models.data(); s.p = p; s.opt = opt;
+        float t3[3], a[kMaxLayers], g3[3], x0[kMaxN], x1[kMaxN];
+        for (size_t i = b; i < e; ++i) {
+            for (int r = 0; r < 3; ++r) {
+                t3[r] = float(target[3 * i + r]);
+                g3[r] = bg ? float(bg[3 * i + r]) : 0.0f;
+            }
+            for (int l = 0; l < L; ++l) a[l] = alpha ? float(alpha[size_t(L) * i + l]) : 0.0f;
+            for (int k = 0; k < N; ++k) x0[k] = float(initial[size_t(N) * i + k]);
+            s.target = t3; s.alpha = a; s.bg = g3; s.counters = nullptr;
+            s.run(x0, x1);
+            for (int k = 0; k < N; ++k) out[size_t(N) * i + k] = double(x1[k]);
+        }
+    });
+    return 0;
+}
+
 // Tight continuation ("polish") of n converged points `start` (n*4L), with
 // multipliers re-estimated by least squares and initial penalty rho0.
 int orc_polish(const orc_layer* layers, const orc_problem* problem, const orc_options* options, size_t n,

@@ -24,3 +24,30 @@ def test_tiny_input_perturbation_moves_some_pixels_beyond_1e3():
           f"(median move {np.median(moved):.1e})")
     assert np.median(moved) < 1e-5        # most pixels barely move
     assert (moved > 1e-3).sum() >= 1      # but the method's stopping point is not stable
+
+
+def test_the_same_method_in_fp32_agrees_on_about_99_percent():
+    """The oracle's own method run in FP32 arithmetic (no GPU involved)
+    against the same method in FP64: the share of pixels within 1e-3 is about
+    99 %, short of 99.9 % — the gap the CUDA path's FP32 solve shows too."""
+    import ctypes
+    wl = syn.workload("rgb1024_l5", 192, 160)
+    L, n = len(wl.layers), wl.pixels
+    lib = oracle.lib()
+    f = lib.dll.orc_solve_f32
+    dp = ctypes.POINTER(ctypes.c_double)
+    f.argtypes = [ctypes.c_void_p, ctypes.POINTER(oracle.Problem), ctypes.POINTER(oracle.Options), ctypes.c_size_t,
+                  dp, dp, dp, dp, dp, ctypes.c_int]
+    f.restype = ctypes.c_int
+    target = np.ascontiguousarray(wl.image.reshape(n, 3))
+    init = np.ascontiguousarray(np.tile(oracle.initial_first(wl.layers, True), (n, 1)))
+    x32 = np.empty_like(init)
+    prob, opts = oracle.problem(L, False, True), oracle.options()
+    assert f(syn.layer_array(wl.layers), ctypes.byref(prob), ctypes.byref(opts), n, target.ctypes.data_as(dp), None,
+             None, init.ctypes.data_as(dp), x32.ctypes.data_as(dp), 0) == 0
+    x64, _ = oracle.unmix(wl.image, wl.layers)
+    p32 = oracle.pack(x32, L, wl.width, wl.height).reshape(L, n, 4)
+    p64 = oracle.pack(x64, L, wl.width, wl.height).reshape(L, n, 4)
+    within = float((np.abs(p32 - p64).max(axis=(0, 2)) <= 1e-3).mean())
+    print(f"oracle FP32 vs FP64: {within:.4%} of {n} pixels within 1e-3")
+    assert 0.95 < within < 0.999
