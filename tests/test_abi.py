@@ -149,3 +149,18 @@ def test_too_many_layers_rejected():
     wl = syn.generate(4, 4, [0] * 9, (2.0, 3.0), seed=1)
     with pytest.raises(ValueError):
         U.compute_color_unmixing(wl.image, wl.layers)
+
+
+def test_row_range_is_checked_before_any_device_work():
+    # Row ranges outside [0, height] or reversed are rejected before any CUDA
+    # call, so this runs without a GPU; the pointers are never dereferenced.
+    wl = syn.workload("rgb256_l3", 4, 4)
+    arr = syn.layer_array(wl.layers)
+    p = ctypes.c_void_p(16)
+    for b, e in [(-1, 2), (3, 2), (0, 5)]:
+        rc = U.lib.unblending_unmix_device_rows(4, 4, p, arr, 3, ctypes.byref(U.options()),
+                                                ctypes.byref(U.solver_options()), p, None, None, b, e, None, None)
+        assert rc == U.INVALID_ARGUMENT, (b, e)
+        rc = U.lib.unblending_refine_device_rows(4, 4, p, arr, 3, p, ctypes.byref(U.options()),
+                                                 ctypes.byref(U.solver_options()), p, None, None, b, e, None, None)
+        assert rc == U.INVALID_ARGUMENT, (b, e)
