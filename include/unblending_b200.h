@@ -18,9 +18,13 @@ extern "C" {
 
 enum {
     /* FP32 solve; every pixel's result is re-checked in FP64 and pixels that
-     * miss the feasibility tolerance are re-solved in FP64. */
+     * miss the feasibility tolerance are re-solved in FP64. Faster, but the
+     * method stops at its own loose tolerance (5e-3), so where it stops
+     * depends on the arithmetic: about 1 % of pixels land more than 1e-3 from
+     * the reference's FP64 result. */
     UNBLENDING_PRECISION_FP32 = 0,
-    /* FP64 solve throughout (the reference's FP64 arithmetic). */
+    /* The reference's FP64 method and arithmetic (the default): results equal
+     * the reference's FP64 solver's to rounding. */
     UNBLENDING_PRECISION_FP64 = 1
 };
 
@@ -29,7 +33,7 @@ enum {
  * (unblending.cpp:351-353). */
 typedef struct unblending_solver_options {
     uint32_t struct_size;
-    int32_t precision;          /* UNBLENDING_PRECISION_*, default FP32 */
+    int32_t precision;          /* UNBLENDING_PRECISION_*, default FP64 */
     int32_t starts;             /* 1..3 solver starts, default 1 */
     int32_t radius;             /* refinement radius; < 0 selects 60 * min(w, h) / 1000 */
     double epsilon;             /* guided-filter regularizer, default 1e-4 */
@@ -43,9 +47,9 @@ typedef struct unblending_solver_options {
                                    rolled over the layers; 4 history in global memory, rolled, 5 blocks per SM;
                                    5 as 3, with three lanes per pixel where the alphas are pinned (refinement) */
     const struct unblending_mlp* warm_start;  /* first pass: learned start point, NULL = the reference's start.
-                                   With FP32 precision and resolve_misses, pixels the learned start leaves
-                                   unsolved get the plain FP32 solve from the reference's start, and what
-                                   that misses the FP64 re-solve (the plain path's fallback). */
+                                   Pixels the learned start leaves unsolved get the plain solve from the
+                                   reference's start (FP64 precision: the FP64 solve; FP32 precision with
+                                   resolve_misses: the FP32 solve, and what that misses the FP64 re-solve). */
     int32_t fp64_variant;       /* FP64 solve and re-solve: -1 default; history in shared memory with 0
                                    uncapped registers, 1 capped for 2 blocks per SM; 2 history in global memory,
                                    x/g/d in shared memory, evaluation rolled, 3 blocks per SM; 3 as 2 with the
@@ -65,7 +69,8 @@ typedef struct unblending_solver_options {
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
-    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP32, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, NULL, -1, 9, 3, 4 }
+    { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP64, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, \
+      NULL, -1, 9, 3, 4 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the
@@ -123,6 +128,9 @@ typedef struct unblending_stats {
     int64_t failed;             /* pixels still missing it at the end */
     int64_t normalization_failed; /* refinement: pixels whose targets could not be normalized */
     double ms_upload, ms_filter, ms_solve, ms_resolve, ms_download, ms_total;
+    /* Evaluations of the call's solves over all pixels, with a value and with
+     * a gradient: of the FP64 solves, and of the FP32 solve. */
+    int64_t fp64_values, fp64_gradients, fp32_values, fp32_gradients;
 } unblending_stats;
 
 /* unblending_unmix / unblending_refine with solver options, an optional
@@ -158,7 +166,8 @@ UNBLENDING_API int32_t unblending_refine_device(
     double* output, int32_t* status, uint32_t* counters, void* stream, unblending_stats* stats);
 
 /* The same two passes restricted to the pixels of rows [row_begin, row_end)
- * of the image (0 <= row_begin <= row_end <= height): only their outputs,
+ * of the image (0 <= row_begin <= row_end <= height, else
+ * UNBLENDING_INVALID_ARGUMENT): only their outputs,
  * status and counters are written. The refinement's guided filter still
  * covers the whole image and reads the whole first pass, so a band's results
  * equal the whole-image call's for its rows bit for bit: an image split into
@@ -186,15 +195,20 @@ UNBLENDING_API int32_t unblending_refine_device_rows(
  * buffers (device memory). The solve's scratch (queue heads, miss counters,
  * miss lists) lives in a fixed 32 MiB + 256 B device array that every GPU
  * loading the library holds until the process exits; images larger than
- * 2048 * 2048 = 4,194,304 pixels return UNBLENDING_INVALID_ARGUMENT. Kernel
- * variants that keep their L-BFGS history in global memory are replaced by
- * their shared-memory counterparts (same results). The call
+ * 2048 * 2048 = 4,194,304 pixels return UNBLENDING_INVALID_ARGUMENT, and so
+ * does a solver->warm_start (the learned start needs buffers of its own).
+ * Kernel variants that keep their L-BFGS history in global memory are
+ * replaced by their shared-memory counterparts: the same results, but the
+ * FP64 solves run slower than unblending_unmix_device's (about 1.7x on the
+ * FP64 re-solve of a 1024x1024 five-layer image). The call
  * uses no cudaMalloc, cudaFree, library stream or event; work is enqueued on
  * `stream` (NULL: the legacy default stream) and the call returns without
  * synchronizing. The first call on a device resolves the array's device
- * address (cudaGetSymbolAddress) and should come before any stream capture.
- * Every call shares the one array, so calls whose GPU work overlaps (several
- * streams, or several host threads) race and must be serialized by the caller. */
+ * address (cudaGetSymbolAddress) and should come before any stream capture;
+ * the address is kept for the process, so calls after a cudaDeviceReset of
+ * that device are not supported. Every call shares the one array, so calls
+ * whose GPU work overlaps (several streams, or several host threads) race and
+ * must be serialized by the caller. */
 UNBLENDING_API int32_t unblending_unmix_device_noalloc(
     int32_t width, int32_t height, const double* image, const unblending_layer* layers, size_t layer_count,
     const unblending_options* options, const unblending_solver_options* solver,

@@ -25,7 +25,7 @@
 //   * refinement targets, normalization .......... unblending/src/unblending.cpp:311-439,
 //                                                    unblending/src/cuda/refinement/filtered_matte_targets.cuh:119-144
 //
-// Parity pin: oracle/build_ref.sh compiles the reference's own host-capable
+// Parity pin: oracle/Makefile (target ref) compiles the reference's own host-capable
 // headers into oracle/_ref/libunbref.so; tests/golden/make_golden.py records
 // its outputs as fixtures, and tests/test_oracle_golden.py checks this oracle
 // against them (bit-exact for blend/evaluate/solve, 1e-12 for the filter).
@@ -444,7 +444,7 @@ template <class T> struct Solver {
     // Least-squares multiplier estimate at x: min |grad E_F - J_F^T lambda|
     // over the variables F strictly inside their bounds.
     void estimate_multipliers() {
-        T gE[kMaxN], J[kMaxC][kMaxN], zero[kMaxC], tmp[kMaxN];
+        T gE[kMaxN], J[kMaxC][kMaxN], zero[kMaxC] = {}, tmp[kMaxN];
         for (int r = 0; r < C; ++r) zero[r] = T(0);
         T e;
         evaluate(models, p, x, target, alpha, zero, T(0), prefix, residual, gE, true, &e);

@@ -1,7 +1,7 @@
 // Thin C shim over the reference's CPU twin of its streaming guided filter.
 //
 // TEST INFRASTRUCTURE ONLY. Compiled as host code by nvcc (the header pulls
-// in CUB) by oracle/build_ref.sh against the reference sources where they lie;
+// in CUB) by oracle/Makefile (target ref) against the reference sources where they lie;
 // linked into oracle/_ref/libunbref.so. Wraps
 //   general::StreamingFilterCPU<double>   refinement/streaming_guided_filter.cuh:92-112
 // which produces the clipped, normalized refinement targets.

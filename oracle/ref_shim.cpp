@@ -1,6 +1,6 @@
 // Thin C shim over the reference's own host-capable solver headers.
 //
-// TEST INFRASTRUCTURE ONLY. oracle/build_ref.sh compiles this file against
+// TEST INFRASTRUCTURE ONLY. oracle/Makefile (target ref) compiles this file against
 // the reference sources where they lie (unblending/src/cuda, included by
 // path) into oracle/_ref/libunbref.so. It is the pin for the oracle
 // restatement in oracle.hpp: tests/golden/make_golden.py records its outputs.

@@ -145,6 +145,20 @@ def test_noalloc_rejects_images_beyond_its_scratch_before_any_device_work():
     assert rc == U.INVALID_ARGUMENT
 
 
+def test_noalloc_rejects_a_learned_start_before_any_device_work():
+    # The allocation-free first pass cannot hold the network or its
+    # predictions, so a warm start is refused (not silently ignored) before
+    # any CUDA call; the pointers are never dereferenced.
+    wl = syn.workload("rgb256_l3", 4, 4)
+    arr = syn.layer_array(wl.layers)
+    net = U.Mlp.new()
+    net.layer_count = 3
+    rc = U.lib.unblending_unmix_device_noalloc(4, 4, ctypes.c_void_p(16), arr, 3, ctypes.byref(U.options()),
+                                               ctypes.byref(U.solver_options(warm_start=net)), ctypes.c_void_p(16),
+                                               None, None)
+    assert rc == U.INVALID_ARGUMENT
+
+
 def test_too_many_layers_rejected():
     wl = syn.generate(4, 4, [0] * 9, (2.0, 3.0), seed=1)
     with pytest.raises(ValueError):
@@ -157,10 +171,45 @@ def test_row_range_is_checked_before_any_device_work():
     wl = syn.workload("rgb256_l3", 4, 4)
     arr = syn.layer_array(wl.layers)
     p = ctypes.c_void_p(16)
-    for b, e in [(-1, 2), (3, 2), (0, 5)]:
+    for b, e in [(-1, 2), (3, 2), (0, 5), (0, -5), (3, -7)]:
         rc = U.lib.unblending_unmix_device_rows(4, 4, p, arr, 3, ctypes.byref(U.options()),
                                                 ctypes.byref(U.solver_options()), p, None, None, b, e, None, None)
         assert rc == U.INVALID_ARGUMENT, (b, e)
         rc = U.lib.unblending_refine_device_rows(4, 4, p, arr, 3, p, ctypes.byref(U.options()),
                                                  ctypes.byref(U.solver_options()), p, None, None, b, e, None, None)
         assert rc == U.INVALID_ARGUMENT, (b, e)
+
+
+def _fault_run(kind):
+    """A child process (the fault is read from its environment) that calls the
+    v1 first pass with the fault injected; prints the code and whether the
+    output buffer was left untouched."""
+    import subprocess
+    import sys
+    code = (
+        "import ctypes, numpy as np\n"
+        "import unblending_b200 as U\n"
+        "from unblending_b200 import synthetic as syn\n"
+        "wl = syn.workload('rgb256_l3', 8, 6)\n"
+        "view, keep = U._view(wl.image)\n"
+        "arr = syn.layer_array(wl.layers)\n"
+        "out = np.full((3, 6, 8, 4), 7.0)\n"
+        "rc = U.lib.unblending_unmix(ctypes.byref(view), arr, 3, None,\n"
+        "                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)\n"
+        "print(rc, bool((out == 7.0).all()))\n"
+    )
+    env = dict(os.environ, UNBLENDING_FAULT=kind)
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    rc, untouched = r.stdout.split()
+    return int(rc), untouched == "True"
+
+
+@pytest.mark.parametrize("kind,expect", [("alloc", U.OUT_OF_MEMORY), ("launch", U.CUDA_ERROR)])
+def test_injected_faults_map_to_their_codes(kind, expect):
+    # A device allocation failure and a kernel launch failure, injected on the
+    # host before any CUDA call (no GPU involved), come back as the
+    # reference's codes (sdk/unblending_c.cpp:87-91) and leave the output
+    # buffer as it was (written only on success).
+    rc, untouched = _fault_run(kind)
+    assert rc == expect and untouched

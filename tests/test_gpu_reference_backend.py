@@ -3,8 +3,10 @@ built for sm_100a by `make -C oracle refgpu`) on the same GPU: the existing
 GPU implementation this path replaces. It runs a different first-pass method
 (FP32 feasibility heuristics, then an FP64 repair with three starts) and
 allocates, uploads and downloads on every call, so the comparison is of the
-two implementations end to end on host buffers: both passes of the 1024x1024
-five-layer image. Skipped where that library was not built.
+two implementations end to end on host buffers, each pass timed on its own:
+the 1024x1024 five-layer image. Both first passes are also compared with the
+oracle (the reference's FP64 solver restated) on a pixel sample. Skipped
+where that library was not built.
 """
 import ctypes
 import os
@@ -13,6 +15,8 @@ import time
 import numpy as np
 import pytest
 
+import oracle
+from tests.parity import report
 from unblending_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -32,6 +36,25 @@ def _planar(packed, L, n):
     return out
 
 
+def _packed(planar, L, n):
+    """The reference's planes -> packed (L, n, 4)."""
+    out = np.empty((L, n, 4))
+    for l in range(L):
+        out[l, :, 3] = planar[l * n:(l + 1) * n]
+        for r in range(3):
+            out[l, :, r] = planar[(L + 3 * l + r) * n:(L + 3 * l + r + 1) * n]
+    return out
+
+
+def _best(f, reps=2):
+    t = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        f()
+        t = min(t, time.perf_counter() - t0)
+    return t
+
+
 @pytest.mark.skipif(not os.path.exists(REF_GPU), reason="oracle/_ref/libunbrefgpu.so not built")
 def test_against_the_reference_cuda_backend(cuda):
     wl = syn.workload("rgb1024_l5", seed=syn.WORKLOADS["rgb1024_l5"]["seed"])
@@ -43,33 +66,51 @@ def test_against_the_reference_cuda_backend(cuda):
     lib.ref_gpu_solve.restype = ctypes.c_int
     layers = syn.layer_array(wl.layers)
     rgb = np.ascontiguousarray(wl.image.reshape(n, 3).T)
-    out = np.zeros(4 * L * n)
+    ref_first = np.zeros(4 * L * n)
+    ref_final = np.zeros(4 * L * n)
     err = ctypes.create_string_buffer(512)
+    codes = {}
 
-    def ours():
-        first = cuda.compute_color_unmixing(wl.image, wl.layers, True)
-        return first, cuda.perform_matte_refinement(wl.image, first, wl.layers, True, True)
+    ours = {}
 
-    first, final = ours()   # warm-up
-    planar_first = _planar(first, L, n)
-    codes = []
+    def our_first():
+        ours["first"] = cuda.compute_color_unmixing(wl.image, wl.layers, True)
 
-    def reference():
-        codes.clear()
-        codes.append(lib.ref_gpu_solve(w, h, layers, L, rgb.ctypes.data_as(dp), None, 1, 0, out.ctypes.data_as(dp),
-                                       err, len(err)))
-        codes.append(lib.ref_gpu_solve(w, h, layers, L, rgb.ctypes.data_as(dp), planar_first.ctypes.data_as(dp), 1, 1,
-                                       out.ctypes.data_as(dp), err, len(err)))
+    def our_refine():
+        ours["final"] = cuda.perform_matte_refinement(wl.image, ours["first"], wl.layers, True, True)
 
-    reference()   # warm-up
-    t_ref = t_ours = float("inf")
-    for _ in range(2):
-        t0 = time.perf_counter(); reference(); t_ref = min(t_ref, time.perf_counter() - t0)
-        t0 = time.perf_counter(); ours(); t_ours = min(t_ours, time.perf_counter() - t0)
+    our_first(); our_refine()   # warm-up
+    planar_first = _planar(ours["first"], L, n)
+
+    def ref_first_pass():
+        codes["first"] = lib.ref_gpu_solve(w, h, layers, L, rgb.ctypes.data_as(dp), None, 1, 0,
+                                           ref_first.ctypes.data_as(dp), err, len(err))
+
+    def ref_refine():
+        # From this path's first pass, so that both refinements see the same input.
+        codes["refine"] = lib.ref_gpu_solve(w, h, layers, L, rgb.ctypes.data_as(dp), planar_first.ctypes.data_as(dp),
+                                            1, 1, ref_final.ctypes.data_as(dp), err, len(err))
+
+    ref_first_pass(); ref_refine()   # warm-up
+    t = {"ref_first": _best(ref_first_pass), "ours_first": _best(our_first),
+         "ref_refine": _best(ref_refine), "ours_refine": _best(our_refine)}
     # 0: solved; 2: the backend's own check rejected an unsolvable pixel after
     # doing all the work (it reports no output then).
-    assert all(c in (0, 2) for c in codes), (codes, err.value)
-    print(f"both passes, host buffers: reference CUDA backend {t_ref:.3f} s ({n / t_ref:.0f} px/s, codes {codes}); "
-          f"this path {t_ours:.3f} s ({n / t_ours:.0f} px/s); speed-up {t_ref / t_ours:.1f}x")
-    assert np.isfinite(final).all()
-    assert t_ours < t_ref
+    assert all(c in (0, 2) for c in codes.values()), (codes, err.value)
+    print("host buffers, seconds:", {k: round(v, 4) for k, v in t.items()}, "codes", codes,
+          "speed-up first pass %.1fx, refinement %.1fx" % (t["ref_first"] / t["ours_first"],
+                                                          t["ref_refine"] / t["ours_refine"]))
+
+    # Both first passes against the oracle on a seeded sample.
+    rng = np.random.default_rng(3)
+    idx = np.sort(rng.choice(n, size=4096, replace=False))
+    x, _ = oracle.unmix(wl.image.reshape(n, 1, 3)[idx], wl.layers)
+    ora = oracle.pack(x, L, len(idx), 1)
+    mine = report(ours["first"].reshape(L, n, 4)[:, idx].reshape(L, 1, len(idx), 4), ora, wl.layers, False)
+    print("this path's first pass vs the oracle:", mine)
+    assert mine["frac_rgba_1e-3"] >= 0.999 and mine["frac_objective"] >= 0.999
+    if codes["first"] == 0:
+        theirs = report(_packed(ref_first, L, n)[:, idx].reshape(L, 1, len(idx), 4), ora, wl.layers, False)
+        print("the reference CUDA backend's first pass vs the oracle:", theirs)
+    assert np.isfinite(ours["final"]).all()
+    assert t["ours_first"] < t["ref_first"] and t["ours_refine"] < t["ref_refine"]

@@ -48,6 +48,18 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda, precision):
         assert np.array_equal(status, ref_status)
 
 
+def test_noalloc_eight_layers_fp64(cuda):
+    # The largest shared-memory slice of the kernels this entry point runs:
+    # eight layers with the FP64 solve (history in shared memory).
+    import torch
+    from unblending_b200 import synthetic as syn
+    wl = syn.generate(40, 32, [0, 1, 2, 3, 9, 5, 8, 11], (4.0, 10.0), seed=58)
+    ref, ref_status, outs = _run(cuda, torch, wl, cuda.solver_options(precision=1))
+    for out, status in outs:
+        np.testing.assert_allclose(out, ref, atol=1e-12, rtol=0)
+        assert np.array_equal(status, ref_status)
+
+
 def test_noalloc_second_image_after_first(cuda):
     import torch
     from unblending_b200 import synthetic as syn

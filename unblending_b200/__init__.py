@@ -11,7 +11,9 @@ reference's buffer API (unblending/include/unblending/pixels.hpp:34-44):
 with the same argument meaning and the same errors (ValueError for
 UNBLENDING_INVALID_ARGUMENT / BUFFER_TOO_SMALL, MemoryError for
 OUT_OF_MEMORY, ExecutionError for CUDA_ERROR / SOLVER_ERROR). There is no CPU
-path: importing this package fails loudly if the CUDA library is missing.
+path: the library is loaded on first use (`lib`, or any call), and that
+fails loudly if the CUDA library is missing. The data helpers of the package
+(`synthetic`, `io`) need no library.
 """
 from __future__ import annotations
 
@@ -101,7 +103,9 @@ class Stats(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_uint32), ("radius", ctypes.c_int32), ("pixels", ctypes.c_int64),
                 ("misses", ctypes.c_int64), ("failed", ctypes.c_int64), ("normalization_failed", ctypes.c_int64),
                 ("ms_upload", ctypes.c_double), ("ms_filter", ctypes.c_double), ("ms_solve", ctypes.c_double),
-                ("ms_resolve", ctypes.c_double), ("ms_download", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_resolve", ctypes.c_double), ("ms_download", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("fp64_values", ctypes.c_int64), ("fp64_gradients", ctypes.c_int64),
+                ("fp32_values", ctypes.c_int64), ("fp32_gradients", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "struct_size"}
@@ -111,10 +115,11 @@ def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> O
     return Options(ctypes.sizeof(Options), backend, int(opaque), int(smooth), concurrency)
 
 
-def solver_options(precision=PRECISION_FP32, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
+def solver_options(precision=PRECISION_FP64, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
                    outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0,
                    kernel_variant=-1, warm_start=None, fp64_variant=-1, fp32_outer=9,
                    gradient_quorum=3, frozen_stop=4) -> SolverOptions:
+    """unblending_solver_options with UNBLENDING_SOLVER_OPTIONS_INIT's defaults."""
     so = SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
                        outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant,
                        ctypes.addressof(warm_start) if warm_start is not None else None, fp64_variant, fp32_outer,
@@ -186,7 +191,22 @@ def _load():
     return lib
 
 
-lib = _load()
+_LIB = None
+
+
+def _lib():
+    """The loaded C-ABI library (loaded on the first call)."""
+    global _LIB
+    if _LIB is None:
+        _LIB = _load()
+    return _LIB
+
+
+def __getattr__(name):
+    # `unblending_b200.lib`: the library, loaded on first access.
+    if name == "lib":
+        return _lib()
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 def _check(rc: int):
@@ -225,7 +245,7 @@ def unmix_ex(image, layers, opaque=True, solver=None, backend=BACKEND_AUTO, with
     status = np.empty(h * w, np.int32) if with_status else None
     counters = np.empty((h * w, 5), np.uint32) if with_counters else None
     stats = Stats(); stats.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_unmix_ex(ctypes.byref(view), arr, L, ctypes.byref(options(opaque, False, backend)),
+    rc = _lib().unblending_unmix_ex(ctypes.byref(view), arr, L, ctypes.byref(options(opaque, False, backend)),
                                  ctypes.byref(solver or solver_options()),
                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size,
                                  status.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if status is not None else None,
@@ -246,7 +266,7 @@ def refine_ex(image, first, layers, opaque=True, smooth=False, solver=None, back
     status = np.empty(h * w, np.int32) if with_status else None
     counters = np.empty((h * w, 5), np.uint32) if with_counters else None
     stats = Stats(); stats.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_refine_ex(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+    rc = _lib().unblending_refine_ex(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                   first.size, ctypes.byref(options(opaque, smooth, backend)),
                                   ctypes.byref(solver or solver_options()),
                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size,
@@ -263,7 +283,7 @@ def compute_color_unmixing(image, layer_infos, has_opaque_background=True, targe
     arr, L = _layers(layer_infos)
     h, w = keep.shape[:2]
     out = np.empty((L, h, w, 4))
-    rc = lib.unblending_unmix(ctypes.byref(view), arr, L,
+    rc = _lib().unblending_unmix(ctypes.byref(view), arr, L,
                               ctypes.byref(options(has_opaque_background, False, BACKEND_AUTO, target_concurrency)),
                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
     _check(rc)
@@ -278,7 +298,7 @@ def perform_matte_refinement(image, layers, layer_infos, has_opaque_background=T
     h, w = keep.shape[:2]
     first = np.ascontiguousarray(layers, dtype=np.float64)
     out = np.empty((L, h, w, 4))
-    rc = lib.unblending_refine(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+    rc = _lib().unblending_refine(ctypes.byref(view), arr, L, first.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                first.size, ctypes.byref(options(has_opaque_background, force_smooth_background,
                                                                 BACKEND_AUTO, target_concurrency)),
                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size)
@@ -291,7 +311,7 @@ def unmix_device(width, height, d_image, layers, d_output, opaque=True, solver=N
     """Device-resident first pass on raw device pointers (ints). Returns stats dict or None."""
     arr, L = _layers(layers)
     st = Stats(); st.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_unmix_device(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+    rc = _lib().unblending_unmix_device(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
                                      ctypes.byref(solver or solver_options()), d_output, d_status, d_counters, stream,
                                      ctypes.byref(st) if stats else None)
     _check(rc)
@@ -303,7 +323,7 @@ def refine_device(width, height, d_image, layers, d_first, d_output, opaque=True
     """Device-resident refinement on raw device pointers (ints). Returns stats dict or None."""
     arr, L = _layers(layers)
     st = Stats(); st.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_refine_device(width, height, d_image, arr, L, d_first, ctypes.byref(options(opaque, smooth)),
+    rc = _lib().unblending_refine_device(width, height, d_image, arr, L, d_first, ctypes.byref(options(opaque, smooth)),
                                       ctypes.byref(solver or solver_options()), d_output, d_status, d_counters, stream,
                                       ctypes.byref(st) if stats else None)
     _check(rc)
@@ -315,7 +335,7 @@ def unmix_device_rows(width, height, d_image, layers, d_output, row_begin, row_e
     """unmix_device restricted to rows [row_begin, row_end) of the image."""
     arr, L = _layers(layers)
     st = Stats(); st.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_unmix_device_rows(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+    rc = _lib().unblending_unmix_device_rows(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
                                           ctypes.byref(solver or solver_options()), d_output, d_status, d_counters,
                                           row_begin, row_end, stream, ctypes.byref(st) if stats else None)
     _check(rc)
@@ -328,7 +348,7 @@ def refine_device_rows(width, height, d_image, layers, d_first, d_output, row_be
     the whole image (d_first must hold the whole first pass)."""
     arr, L = _layers(layers)
     st = Stats(); st.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_refine_device_rows(width, height, d_image, arr, L, d_first,
+    rc = _lib().unblending_refine_device_rows(width, height, d_image, arr, L, d_first,
                                            ctypes.byref(options(opaque, smooth)),
                                            ctypes.byref(solver or solver_options()), d_output, d_status, d_counters,
                                            row_begin, row_end, stream, ctypes.byref(st) if stats else None)
@@ -342,7 +362,7 @@ def unmix_device_noalloc(width, height, d_image, layers, d_output, opaque=True, 
     library; up to 2048*2048 pixels). For callers that cannot allocate during
     processing. Calls that overlap on the GPU race on the shared scratch."""
     arr, L = _layers(layers)
-    rc = lib.unblending_unmix_device_noalloc(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
+    rc = _lib().unblending_unmix_device_noalloc(width, height, d_image, arr, L, ctypes.byref(options(opaque)),
                                              ctypes.byref(solver or solver_options()), d_output, d_status, stream)
     _check(rc)
 
@@ -358,7 +378,7 @@ def mlp_train_device(images, layers, solver=None, batch=8192, steps=512, learnin
     hs = (ctypes.c_int32 * k)(*[h for _, _, h in images])
     mo = MlpOptions(ctypes.sizeof(MlpOptions), batch, steps, learning_rate, seed)
     model = Mlp.new()
-    _check(lib.unblending_mlp_train_device(k, ws, hs, ptrs, arr, L, ctypes.byref(options(opaque)),
+    _check(_lib().unblending_mlp_train_device(k, ws, hs, ptrs, arr, L, ctypes.byref(options(opaque)),
                                            ctypes.byref(solver or solver_options()), ctypes.byref(mo),
                                            ctypes.byref(model)))
     return model
@@ -366,12 +386,12 @@ def mlp_train_device(images, layers, solver=None, batch=8192, steps=512, learnin
 
 def mlp_loss_grad_device(model: Mlp, count, d_features, d_targets) -> Mlp:
     grad = Mlp.new()
-    _check(lib.unblending_mlp_loss_grad_device(ctypes.byref(model), count, d_features, d_targets, ctypes.byref(grad)))
+    _check(_lib().unblending_mlp_loss_grad_device(ctypes.byref(model), count, d_features, d_targets, ctypes.byref(grad)))
     return grad
 
 
 def mlp_predict_device(model: Mlp, width, height, d_image, d_out, stream=None):
-    _check(lib.unblending_mlp_predict_device(ctypes.byref(model), width, height, d_image, d_out, stream))
+    _check(_lib().unblending_mlp_predict_device(ctypes.byref(model), width, height, d_image, d_out, stream))
 
 
 def unmix_batch_device(jobs, opaque=True, solver=None, stream=None, stats=False):
@@ -388,7 +408,7 @@ def unmix_batch_device(jobs, opaque=True, solver=None, stream=None, stats=False)
         arr[k] = ImageJob(j["width"], j["height"], j["d_image"], ctypes.addressof(layers), L, j["d_output"],
                           j.get("d_status"), ctypes.addressof(warm) if warm is not None else None)
     st = Stats(); st.struct_size = ctypes.sizeof(Stats)
-    rc = lib.unblending_unmix_batch_device(arr, len(jobs), ctypes.byref(options(opaque)),
+    rc = _lib().unblending_unmix_batch_device(arr, len(jobs), ctypes.byref(options(opaque)),
                                            ctypes.byref(solver or solver_options()), stream,
                                            ctypes.byref(st) if stats else None)
     _check(rc)
@@ -396,4 +416,4 @@ def unmix_batch_device(jobs, opaque=True, solver=None, stream=None, stats=False)
 
 
 def last_launch_count() -> int:
-    return int(lib.unblending_last_launch_count())
+    return int(_lib().unblending_last_launch_count())

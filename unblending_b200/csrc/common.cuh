@@ -107,6 +107,8 @@ struct SolveArgs {
     const BatchJob* jobs = nullptr;
     int job_count = 0;
     const void* models = nullptr;
+    // Optional totals over the launch: evaluations with a value, with a gradient.
+    unsigned long long* tally = nullptr;
     int opaque = 1, smooth = 0;
     // Global-memory L-BFGS history (kernels that keep it there): room for
     // history_lanes lanes; the launch uses at most history_lanes / 128 blocks.

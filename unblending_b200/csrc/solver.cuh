@@ -281,6 +281,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     Group<kLanes> Q;
     bool colour, opaque, smooth;
     T tol2, itol;
+    // Evaluations of this lane's pixels (lane q = 0 counts), with a value and
+    // with a gradient, for SolveArgs::tally.
+    uint32_t n_value = 0, n_grad = 0;
 
     // Current pixel (this lane's slice of it).
     int pixel = 0, gidx = 0;   // pixel index within its image, queue index
@@ -461,6 +464,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if (active) {
             count(0);
             if (need_grad) count(1);
+            if (Q.q == 0) { ++n_value; if (need_grad) ++n_grad; }
             const bool feasible = norm < tol2;
             if (finite_(energy) && finite_(norm) &&
                 (!have_best || (feasible && (best_norm >= tol2 || energy < best_energy)) ||
@@ -1270,6 +1274,14 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             }
             const T value = Q.extra ? T(0) : evaluate(need_grad && go, go);
             if (go) act = after_evaluation(value, need_grad);
+        }
+        if (a.tally) {
+            // One atomic per warp and count.
+            const uint32_t v = __reduce_add_sync(0xffffffffu, n_value), g = __reduce_add_sync(0xffffffffu, n_grad);
+            if ((threadIdx.x & 31) == 0) {
+                atomicAdd(a.tally + 0, (unsigned long long)v);
+                atomicAdd(a.tally + 1, (unsigned long long)g);
+            }
         }
     }
 };

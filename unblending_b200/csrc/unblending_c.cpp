@@ -7,6 +7,7 @@
 // same validation order, same error codes, output written only on success.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -385,8 +386,15 @@ struct PassIO {
 
 struct PassResult {
     int32_t* small = nullptr;   // device: [0] misses, [1] failures after re-solve, [2] normalization failures
+    unsigned long long* tally = nullptr;   // device: SolveArgs::tally of the FP64 solves, then of the FP32 solve
     int radius = 0;
 };
+
+// Totals of a pass's evaluations (PassResult::tally) into the stats.
+void put_tally(unblending_stats* st, const unsigned long long* t) {
+    st->fp64_values = int64_t(t[0]); st->fp64_gradients = int64_t(t[1]);
+    st->fp32_values = int64_t(t[2]); st->fp32_gradients = int64_t(t[3]);
+}
 
 // Enqueues one pass on `s`. Events ev[0..3] bracket filter / solve / re-solve.
 PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblending_layer* layers,
@@ -394,10 +402,13 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     PassResult R;
     const int L = sp.layers;
     const size_t n = sp.pixels;
-    uint32_t* queues = c.small.get<uint32_t>(8);
+    // Words [0, 4) queue heads, [4, 8) counts, then 4 tally totals (64-bit):
+    // FP64 values, FP64 gradients, FP32 values, FP32 gradients.
+    uint32_t* queues = c.small.get<uint32_t>(8 + 8);
     int32_t* counts = reinterpret_cast<int32_t*>(queues + 4);
     R.small = counts;
-    ck(cudaMemsetAsync(queues, 0, 8 * sizeof(uint32_t), s));
+    R.tally = reinterpret_cast<unsigned long long*>(queues + 8);
+    ck(cudaMemsetAsync(queues, 0, (8 + 8) * sizeof(uint32_t), s));
 
     ck(cudaEventRecord(c.ev[0], s));
     double* targets = nullptr;
@@ -428,6 +439,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     a.queue = queues;
     a.miss_list = c.list_a.get<int32_t>(n);
     a.miss_count = counts + 0;
+    a.tally = R.tally;
     if (!refine && so.warm_start) {
         // Learned start point for every pixel, then the solve from it.
         const MlpDevice dev = upload_model(c, *so.warm_start, s);
@@ -442,13 +454,29 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     void* history = c.history.get<unsigned char>(history_bytes(L, sizeof(double), c.sms));
     if (so.precision == UNBLENDING_PRECISION_FP64) {
         attach_history(a, history, true, fp64_variant(so, refine), c.sms);
-        ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads, c.sms, s));
+        ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads,
+                             c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
-        ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+        if (a.warm) {
+            // Pixels that the learned start leaves unsolved get the plain
+            // solve from the reference's start.
+            SolveArgs b = a;
+            b.list = a.miss_list; b.list_count = counts + 0;
+            b.miss_list = c.list_b.get<int32_t>(n); b.miss_count = counts + 1;
+            b.queue = queues + 1;
+            b.input_status = nullptr; b.input_failed = nullptr;
+            b.warm = nullptr;
+            ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, b, threads,
+                                 c.sms, s));
+            ++t_launches;
+        } else {
+            ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+        }
     } else {
         const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, refine);
         attach_history(a, history, false, variant, c.sms);
+        a.tally = R.tally + 2;
         ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
@@ -482,8 +510,10 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
             b.input_status = nullptr; b.input_failed = nullptr;
             b.warm = nullptr;   // the reference's (cold) start
             b.history = nullptr; b.history_lanes = 0;
+            b.tally = R.tally;
             attach_history(b, history, true, fp64_variant(so, refine), c.sms);
-            ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl_re, b, threads, c.sms, s));
+            ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl_re, b,
+                                 threads, c.sms, s));
             ++t_launches;
         } else {
             ck(cudaMemcpyAsync(counts + 1, counts + 0, sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
@@ -498,8 +528,22 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? ms : 0.f;
 }
 
+// Host-side fault injection (no GPU fault): UNBLENDING_FAULT=alloc makes the
+// call fail as a device allocation does (ck's std::bad_alloc),
+// UNBLENDING_FAULT=launch as a failed kernel launch does (ck's CudaFailure),
+// before its first CUDA call; the call then returns UNBLENDING_OUT_OF_MEMORY /
+// UNBLENDING_CUDA_ERROR without touching the device or the caller's output
+// (sdk/unblending_c.cpp:87-91 maps exceptions to these codes).
+void injected_fault() {
+    const char* f = std::getenv("UNBLENDING_FAULT");
+    if (!f) return;
+    if (std::strcmp(f, "alloc") == 0) throw std::bad_alloc();
+    if (std::strcmp(f, "launch") == 0) throw CudaFailure(cudaErrorLaunchFailure);
+}
+
 template <class F> int32_t guarded(F&& f) {
     try {
+        injected_fault();
         return f();
     } catch (const std::bad_alloc&) { return UNBLENDING_OUT_OF_MEMORY; }
     catch (const CudaFailure& e) { cudaGetLastError(); return UNBLENDING_CUDA_ERROR; }
@@ -552,7 +596,9 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
         io.counters = counters ? c.counters.get<uint32_t>(5 * n) : nullptr;
         PassResult R = enqueue_pass(c, sp, refine, layers, so, io, s);
         int32_t counts[3] = {0, 0, 0};
+        unsigned long long tally[4] = {};
         ck(cudaMemcpyAsync(counts, R.small, sizeof(counts), cudaMemcpyDeviceToHost, s));
+        ck(cudaMemcpyAsync(tally, R.tally, sizeof(tally), cudaMemcpyDeviceToHost, s));
         ck(cudaStreamSynchronize(s));
         if (sp.strict && (counts[1] > 0 || counts[2] > 0)) throw SolverFailure("pixels miss the feasibility tolerance");
         ck(cudaEventRecord(c.ev[4], s));
@@ -574,6 +620,7 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
             stats->ms_resolve = elapsed(c.ev[2], c.ev[3]);
             stats->ms_download = elapsed(c.ev[4], t1);
             stats->ms_total = elapsed(t0, t1);
+            put_tally(stats, tally);
         }
         return UNBLENDING_OK;
     });
@@ -617,7 +664,9 @@ int32_t device_call(int32_t width, int32_t height, const double* image, const un
         PassResult R = enqueue_pass(c, sp, refine, layers, so, io, s);
         if (stats) {
             int32_t counts[3] = {0, 0, 0};
+            unsigned long long tally[4] = {};
             ck(cudaMemcpyAsync(counts, R.small, sizeof(counts), cudaMemcpyDeviceToHost, s));
+            ck(cudaMemcpyAsync(tally, R.tally, sizeof(tally), cudaMemcpyDeviceToHost, s));
             ck(cudaStreamSynchronize(s));
             stats->radius = R.radius;
             stats->pixels = int64_t(row_end - row_begin) * width;
@@ -630,6 +679,7 @@ int32_t device_call(int32_t width, int32_t height, const double* image, const un
             stats->ms_resolve = elapsed(c.ev[2], c.ev[3]);
             stats->ms_download = 0;
             stats->ms_total = elapsed(c.ev[0], c.ev[3]);
+            put_tally(stats, tally);
             if (sp.strict && (counts[1] > 0 || counts[2] > 0)) throw SolverFailure("pixels miss the feasibility tolerance");
         }
         ck(cudaPeekAtLastError());
@@ -693,6 +743,7 @@ int32_t unblending_unmix_device_rows(int32_t width, int32_t height, const double
                                      const unblending_options* options, const unblending_solver_options* solver,
                                      double* output, int32_t* status, uint32_t* counters, int32_t row_begin,
                                      int32_t row_end, void* stream, unblending_stats* stats) {
+    if (row_end < 0) return UNBLENDING_INVALID_ARGUMENT;   // (device_call reads -1 as "every row")
     return device_call(width, height, image, layers, layer_count, nullptr, options, solver, output, status, counters,
                        stream, stats, false, row_begin, row_end);
 }
@@ -702,6 +753,7 @@ int32_t unblending_refine_device_rows(int32_t width, int32_t height, const doubl
                                       const unblending_options* options, const unblending_solver_options* solver,
                                       double* output, int32_t* status, uint32_t* counters, int32_t row_begin,
                                       int32_t row_end, void* stream, unblending_stats* stats) {
+    if (row_end < 0) return UNBLENDING_INVALID_ARGUMENT;   // (device_call reads -1 as "every row")
     return device_call(width, height, image, layers, layer_count, first_pass, options, solver, output, status,
                        counters, stream, stats, true, row_begin, row_end);
 }
@@ -1193,6 +1245,9 @@ int32_t unblending_unmix_device_noalloc(int32_t width, int32_t height, const dou
     unblending_solver_options so;
     if ((rc = resolve_solver(solver, so)) != UNBLENDING_OK) return rc;
     if (sp.pixels > noalloc_max_pixels()) return UNBLENDING_INVALID_ARGUMENT;   // checked before any CUDA call
+    // The learned start needs device buffers of its own (network, predictions):
+    // refused here rather than silently ignored.
+    if (so.warm_start) return UNBLENDING_INVALID_ARGUMENT;
     return guarded([&]() -> int32_t {
         void* base = nullptr;
         size_t bytes = 0, max_pixels = 0;
