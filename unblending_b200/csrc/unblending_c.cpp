@@ -894,7 +894,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 b.list = lists; b.list_count = G.counts + 0;
                 b.miss_list = lists + total; b.miss_count = G.counts + 1;
                 b.queue = G.queues + 1;
-                if (!G.infer.empty()) {
+                if (!G.infer.empty() && so.precision != UNBLENDING_PRECISION_FP64) {
                     // As the single-image pass: the learned start's misses get the
                     // plain FP32 solve first (cold jobs of the group repeat theirs,
                     // with the same result), its misses the FP64 re-solve.
@@ -909,7 +909,10 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     b.miss_list = lists;
                 }
                 a.models = so.precision == UNBLENDING_PRECISION_FP64 ? static_cast<const void*>(d_m64) : d_m32;
-                if (so.precision == UNBLENDING_PRECISION_FP64) a.miss_count = G.counts + 1;
+                // FP64: the solve's misses are the group's failures, unless a
+                // learned start leaves them to the plain solve (G.re, as the
+                // single-image pass does).
+                if (so.precision == UNBLENDING_PRECISION_FP64 && G.infer.empty()) a.miss_count = G.counts + 1;
                 plan->counts.push_back(G.counts);
                 plan->pixels += total;
                 void* history = plan->alloc<unsigned char>(history_bytes(L, sizeof(double), c.sms));
@@ -971,6 +974,10 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     if (so.precision == UNBLENDING_PRECISION_FP64) {
                         ck(launch_solve_batch_fp64(G.L, fp64_variant(so, false), ctl, G.fp, 128, c.sms, s));
                         ++launches;
+                        if (!G.infer.empty()) {
+                            ck(launch_solve_batch_fp64(G.L, fp64_variant(so, false), ctl, G.re, 128, c.sms, s));
+                            ++launches;
+                        }
                     } else {
                         ck(launch_solve_batch_fp32(G.L, G.variant, ctl32, G.fp, G.threads, c.sms, s));
                         ++launches;
