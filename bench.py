@@ -108,6 +108,7 @@ def parse():
     p.add_argument("--no-warm", action="store_true")
     p.add_argument("--no-fp32", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the rgb256_l3 / rgb4096_l6 keys")
+    p.add_argument("--fp64-variant", type=int, default=-1, help="FP64 kernel variant of the default solve (-1: tuned)")
     return p.parse_args()
 
 
@@ -536,7 +537,8 @@ def b200_arm(args):
     stream = torch.cuda.Stream()
     D = Decomposition(U, torch, wl, stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    default = U.solver_options(radius=radius)   # UNBLENDING_SOLVER_OPTIONS_INIT, the workload's radius
+    # UNBLENDING_SOLVER_OPTIONS_INIT with the workload's radius.
+    default = U.solver_options(radius=radius, fp64_variant=args.fp64_variant)
 
     sampler = ClockSampler(local)
     if world > 1:

@@ -4,6 +4,8 @@ results, also when the graph is replayed and with a learned start."""
 import numpy as np
 import pytest
 
+import oracle
+from tests.parity import PIXEL_FRACTION, report
 from tests.test_mlp_reference import random_model
 from unblending_b200 import synthetic as syn
 
@@ -59,3 +61,21 @@ def test_batch_with_warm_start_equals_per_image(cuda):
         cuda.unmix_device(w.width, w.height, i.data_ptr(), w.layers, ref.data_ptr(), solver=so)
         torch.cuda.synchronize()
         assert np.array_equal(o.cpu().numpy(), ref.cpu().numpy())
+
+
+def test_batch_matches_oracle(cuda):
+    """The batched first pass (default solve) against the oracle on every
+    image of a small uneven batch (layer counts 3-6, seven modes), to the
+    parity bar."""
+    import torch
+    wls = syn.batch(count=6, seed=12, sides=(24, 56))
+    imgs, outs, sts = _device(torch, wls)
+    jobs = [dict(width=w.width, height=w.height, d_image=i.data_ptr(), layers=w.layers, d_output=o.data_ptr(),
+                 d_status=s.data_ptr()) for w, i, o, s in zip(wls, imgs, outs, sts)]
+    cuda.unmix_batch_device(jobs, stats=True)
+    for w, o in zip(wls, outs):
+        L = len(w.layers)
+        x, _ = oracle.unmix(w.image, w.layers)
+        r = report(o.cpu().numpy().reshape(L, w.height, w.width, 4), oracle.pack(x, L, w.width, w.height), w.layers,
+                   False)
+        assert r["frac_rgba_1e-3"] >= PIXEL_FRACTION and r["frac_objective"] >= PIXEL_FRACTION, (w.name, L, r)

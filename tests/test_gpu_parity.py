@@ -111,16 +111,43 @@ def test_unmix_matches_oracle_rgb1024_l5_crop(cuda, precision):
 
 @pytest.mark.parametrize("mode", range(13))
 def test_every_blend_mode_fp64(cuda, mode):
-    wl = syn.generate(24, 20, [0, mode], (5.0, 20.0), seed=100 + mode)
+    """Every blend mode (blend_mode.hpp:90-196) with the default (FP64)
+    solve, both passes, to the parity bar."""
+    wl = syn.generate(48, 40, [0, mode, 2, mode], (5.0, 20.0), seed=100 + mode)
     ref, _ = oracle_unmix(wl)
-    out, status, _, _ = cuda.unmix_ex(wl.image, wl.layers, solver=solver(cuda, 1))
+    out, status, _, _ = cuda.unmix_ex(wl.image, wl.layers)
     r = report(out, ref, wl.layers, False)
-    assert r["frac_rgba_1e-3"] >= 0.995, r
+    assert r["frac_rgba_1e-3"] >= PIXEL_FRACTION and r["frac_objective"] >= PIXEL_FRACTION, r
     first = ref
     rref, _, _ = oracle_refine(wl, first, smooth=False, radius=2)
-    rout, _, _, _ = cuda.refine_ex(wl.image, first, wl.layers, smooth=False, solver=solver(cuda, 1, radius=2))
+    rout, _, _, _ = cuda.refine_ex(wl.image, first, wl.layers, smooth=False, solver=cuda.solver_options(radius=2))
     rr = report(rout, rref, wl.layers, True)
-    assert rr["frac_rgba_1e-3"] >= 0.995, rr
+    assert rr["frac_rgba_1e-3"] >= PIXEL_FRACTION and rr["frac_objective"] >= PIXEL_FRACTION, rr
+
+
+# Measured agreement of the FP32 solve (table-driven blend) with the oracle
+# per mode on these images: 0.98-1.0 of pixels within 1e-3 in the first pass
+# and in the refinement; the floor sits below.
+FP32_MODE_FLOOR = 0.95
+
+
+@pytest.mark.parametrize("mode", range(13))
+def test_every_blend_mode_fp32_table(cuda, mode):
+    """The FP32 solve's table-driven blend (the ten piecewise-bilinear modes
+    by coefficients, Dodge/Burn/SoftLight evaluated directly) for every mode,
+    both passes, against the oracle. FP32 stops where its own arithmetic
+    leads it at the method's 5e-3 tolerance, so it is checked at a floor
+    below the bar; a wrong formula or branch would miss it by far."""
+    wl = syn.generate(48, 40, [0, mode, 2, mode], (5.0, 20.0), seed=100 + mode)
+    ref, _ = oracle_unmix(wl)
+    out, status, _, _ = cuda.unmix_ex(wl.image, wl.layers, solver=solver(cuda, 0))
+    r = report(out, ref, wl.layers, False)
+    first = ref
+    rref, _, _ = oracle_refine(wl, first, smooth=False, radius=2)
+    rout, _, _, _ = cuda.refine_ex(wl.image, first, wl.layers, smooth=False, solver=solver(cuda, 0, radius=2))
+    rr = report(rout, rref, wl.layers, True)
+    print("fp32 mode", mode, r["frac_rgba_1e-3"], rr["frac_rgba_1e-3"])
+    assert r["frac_rgba_1e-3"] >= FP32_MODE_FLOOR and rr["frac_rgba_1e-3"] >= FP32_MODE_FLOOR, (r, rr)
 
 
 def test_plus_stack_non_opaque(cuda):
@@ -315,3 +342,28 @@ def test_frozen_stop_leaves_results_unchanged(cuda, case):
     print("frozen stop case", case, "misses", s1["misses"], s2["misses"])
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_fp64_kernel_variants_are_bit_identical(cuda, case):
+    """The FP64 kernel variants differ only in where their vectors live and
+    how their loops are laid out (history in shared or global memory, the
+    bookkeeping unrolled or rolled over the layers, four or three lanes per
+    pixel): outputs, status and work counters of both passes are identical."""
+    if case == 0:
+        wl, opaque, smooth = syn.workload("rgb1024_l5", 96, 80), True, True
+    elif case == 1:
+        wl, opaque, smooth = syn.generate(64, 48, [0, 6, 7, 9, 1, 2, 8, 11], (4.0, 16.0), seed=91), True, False
+    else:
+        wl, opaque, smooth = syn.generate(64, 48, [0, 1, 2], (4.0, 12.0), seed=7, comp=syn.PLUS), False, False
+    runs = {}
+    for v1, v2 in ((0, 2), (2, 5), (3, 5), (6, 6)):
+        first, st1, c1, _ = cuda.unmix_ex(wl.image, wl.layers, opaque=opaque, with_counters=True,
+                                          solver=solver(cuda, 1, radius=3, fp64_variant=v1))
+        final, st2, c2, _ = cuda.refine_ex(wl.image, first, wl.layers, opaque=opaque, smooth=smooth,
+                                           with_counters=True, solver=solver(cuda, 1, radius=3, fp64_variant=v2))
+        runs[(v1, v2)] = (first, st1, c1, final, st2, c2)
+    base = runs[(3, 5)]
+    for key, outs in runs.items():
+        for a, b in zip(base, outs):
+            assert np.array_equal(a, b), key

@@ -12,16 +12,29 @@
 // require alpha_0 == 1 within 1e-5).
 //
 // Layout: planes of n doubles, row-major pixels. Each mean filter is two
-// sliding-window passes (rows, then columns), O(1) per pixel for any radius.
-// The row pass gives each thread one row (its reads stream through L1); the
-// column pass gives each thread one column so a warp reads 32 adjacent
-// doubles per row step. All sums stay in FP64: E[I^2] - E[I]^2 cancels.
+// passes (rows, then columns), O(1) per pixel for any radius, as the
+// reference's GPU filter is (row prefix scans, guided_filter.cuh:49-66):
+//   * rows: one CTA per image row; each plane of the row is prefix-summed
+//     across the CTA in shared memory (FP64) and the window sums are prefix
+//     differences, read and written with coalesced accesses. The first box's
+//     planes (I, I I^T, p, I p) are formed from the image and the first pass
+//     inside this kernel instead of being packed to memory first.
+//   * columns: one thread per (plane, column, segment of rows) with a
+//     sliding window down its segment, so that a warp reads 32 adjacent
+//     doubles per step and the grid has enough warps to cover the latency.
+// All sums stay in FP64: E[I^2] - E[I]^2 cancels.
 #include "solver_dispatch.hpp"
 
 namespace unb {
 namespace {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+constexpr int kRowThreads = 256;
+// Widest row the prefix pass keeps in shared memory (96 KiB of doubles);
+// wider images take the one-thread-per-row sliding pass.
+constexpr int kRowPrefixMaxWidth = 12288;
+constexpr int kColSegment = 128;   // rows per thread of the column pass
 
 // Channel value p_c of pixel i: first-pass alpha of layer c (c < L), else the
 // background colour channel c - L.
@@ -45,7 +58,100 @@ __global__ void pack_planes(const double* image, const double* first, double* pl
     }
 }
 
-// Sliding mean along rows: one thread per (plane, row).
+// Value of packed plane k (the layout of pack_planes) at pixel i.
+__device__ __forceinline__ double packed_value(const double* image, const double* first, size_t n, int L, int k,
+                                               size_t i) {
+    if (k < 3) return image[3 * i + k];
+    if (k < 9) {
+        // I_r I_r, I_r I_g, I_r I_b, I_g I_g, I_g I_b, I_b I_b
+        const int a = k < 6 ? 0 : (k < 8 ? 1 : 2);
+        const int b = k < 6 ? k - 3 : (k < 8 ? k - 5 : 2);
+        return image[3 * i + a] * image[3 * i + b];
+    }
+    const int c = (k - 9) >> 2, m = (k - 9) & 3;
+    const double p = channel(first, n, L, c, i);
+    return m == 0 ? p : image[3 * i + (m - 1)] * p;
+}
+
+// Clamp-to-edge window mean along rows by prefix sums, one CTA per row:
+// for each plane the row's values go to shared memory, are prefix-summed
+// across the CTA (each thread scans its chunk, the chunk totals are scanned
+// by shuffles), and out[x] = (S[min(x+r, w-1)] - S[x-r-1] + clamped copies of
+// the end values) / (2r+1). PACKED: plane k of the input is packed plane k,
+// formed from the image and the first pass.
+template <bool PACKED>
+__global__ void __launch_bounds__(kRowThreads)
+box_rows_prefix(const double* in, const double* image, const double* first, double* out, int w, int h, int planes,
+                int L, int r) {
+    extern __shared__ double sm_row[];   // w prefix values, then one total per warp
+    double* warp_total = sm_row + w;
+    const int y = blockIdx.x;
+    const size_t n = size_t(w) * h, row0 = size_t(y) * w;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int chunk = (w + kRowThreads - 1) / kRowThreads;
+    const int x0 = min(w, t * chunk), x1 = min(w, x0 + chunk);
+    const double norm = double(2 * r + 1);
+    for (int k = 0; k < planes; ++k) {
+        const double* src = PACKED ? nullptr : in + size_t(k) * n + row0;
+        // Coalesced load of the row into shared memory.
+        for (int x = t; x < w; x += kRowThreads)
+            sm_row[x] = PACKED ? packed_value(image, first, n, L, k, row0 + x) : src[x];
+        __syncthreads();
+        // Inclusive scan: this thread's chunk, then the chunk totals.
+        double s = 0.0;
+        for (int x = x0; x < x1; ++x) { s += sm_row[x]; sm_row[x] = s; }
+        double incl = s;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) warp_total[wid] = incl;
+        __syncthreads();
+        double carry = incl - s;   // exclusive prefix of this thread within its warp
+        for (int q = 0; q < wid; ++q) carry += warp_total[q];
+        for (int x = x0; x < x1; ++x) sm_row[x] += carry;
+        __syncthreads();
+        // Window sums: prefix differences plus the clamped copies of the end
+        // values (read again from their source, exactly).
+        const double first_v = PACKED ? packed_value(image, first, n, L, k, row0) : src[0];
+        const double last_v = PACKED ? packed_value(image, first, n, L, k, row0 + w - 1) : src[w - 1];
+        double* dst = out + size_t(k) * n + row0;
+        for (int x = t; x < w; x += kRowThreads) {
+            const int hi = min(x + r, w - 1), lo = x - r - 1;
+            double sum = sm_row[hi] - (lo >= 0 ? sm_row[lo] : 0.0);
+            if (x - r < 0) sum += double(r - x) * first_v;
+            if (x + r > w - 1) sum += double(x + r - (w - 1)) * last_v;
+            dst[x] = sum / norm;
+        }
+        __syncthreads();
+    }
+}
+
+// Clamp-to-edge window mean along columns: one thread per (plane, column,
+// segment of kColSegment rows), sliding down its segment; the first window
+// is summed in full. Threads of a warp take adjacent columns.
+__global__ void box_cols_segments(const double* in, double* out, int w, int h, int planes, int r) {
+    const int segs = (h + kColSegment - 1) / kColSegment;
+    const size_t job = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (job >= size_t(planes) * segs * w) return;
+    const int x = int(job % w);
+    const size_t rest = job / w;
+    const int s = int(rest % segs), p = int(rest / segs);
+    const double* col = in + size_t(p) * w * h + x;
+    double* o = out + size_t(p) * w * h + x;
+    const int y0 = s * kColSegment, y1 = min(h, y0 + kColSegment);
+    const double norm = double(2 * r + 1);
+    double sum = 0.0;
+    for (int j = y0 - r; j <= y0 + r; ++j) sum += col[size_t(clampi(j, 0, h - 1)) * w];
+    for (int y = y0; y < y1; ++y) {
+        o[size_t(y) * w] = sum / norm;
+        sum += col[size_t(clampi(y + r + 1, 0, h - 1)) * w] - col[size_t(clampi(y - r, 0, h - 1)) * w];
+    }
+}
+
+// Sliding mean along rows: one thread per (plane, row) (rows wider than the
+// prefix pass holds).
 __global__ void box_rows(const double* in, double* out, int w, int h, int planes, int r) {
     const int job = blockIdx.x * blockDim.x + threadIdx.x;
     if (job >= planes * h) return;
@@ -59,24 +165,6 @@ __global__ void box_rows(const double* in, double* out, int w, int h, int planes
     for (int x = 0; x < w; ++x) {
         o[x] = sum / norm;
         sum += row[clampi(x + r + 1, 0, w - 1)] - row[clampi(x - r, 0, w - 1)];
-    }
-}
-
-// Sliding mean along columns: one thread per (plane, column).
-__global__ void box_cols(const double* in, double* out, int w, int h, int planes, int r) {
-    const int job = blockIdx.x * blockDim.x + threadIdx.x;
-    if (job >= planes * w) return;
-    const int p = job / w, x = job % w;
-    const double* col = in + size_t(p) * w * h + x;
-    double* o = out + size_t(p) * w * h + x;
-    const double norm = double(2 * r + 1);
-    double sum = double(r + 1) * col[0];
-    const int hi = r < h - 1 ? r : h - 1;
-    for (int y = 1; y <= hi; ++y) sum += col[size_t(y) * w];
-    if (r >= h) sum += double(r - h + 1) * col[size_t(h - 1) * w];
-    for (int y = 0; y < h; ++y) {
-        o[size_t(y) * w] = sum / norm;
-        sum += col[size_t(clampi(y + r + 1, 0, h - 1)) * w] - col[size_t(clampi(y - r, 0, h - 1)) * w];
     }
 }
 
@@ -135,13 +223,44 @@ __global__ void finish_targets(const double* image, const double* first, const d
     }
 }
 
-void box(const double* in, double* tmp, double* out, int w, int h, int planes, int r, cudaStream_t s) {
-    const int threads = 128;
-    box_rows<<<(planes * h + threads - 1) / threads, threads, 0, s>>>(in, tmp, w, h, planes, r);
-    box_cols<<<(planes * w + threads - 1) / threads, threads, 0, s>>>(tmp, out, w, h, planes, r);
+// Window means of `planes` planes: rows (prefix pass, or the sliding pass
+// for very wide rows) into tmp, then columns into out. With `image`, the
+// input planes are the packed planes of the first box, formed on the fly
+// (the sliding row pass needs them in memory: pack_planes writes them to
+// `in` first).
+cudaError_t box(const double* in, const double* image, const double* first, int L, int channels, double* tmp,
+                double* out, int w, int h, int planes, int r, cudaStream_t s) {
+    if (w <= kRowPrefixMaxWidth) {
+        const size_t smem = (size_t(w) + kRowThreads / 32) * sizeof(double);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(image ? box_rows_prefix<true> : box_rows_prefix<false>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (e != cudaSuccess) return e;
+        }
+        if (image) box_rows_prefix<true><<<h, kRowThreads, smem, s>>>(nullptr, image, first, tmp, w, h, planes, L, r);
+        else box_rows_prefix<false><<<h, kRowThreads, smem, s>>>(in, nullptr, nullptr, tmp, w, h, planes, L, r);
+    } else {
+        const int threads = 128;
+        if (image) {
+            int grid = int((size_t(w) * h + 255) / 256);
+            if (grid > 148 * 32) grid = 148 * 32;
+            pack_planes<<<grid, 256, 0, s>>>(image, first, const_cast<double*>(in), size_t(w) * h, L, channels);
+        }
+        box_rows<<<(planes * h + threads - 1) / threads, threads, 0, s>>>(in, tmp, w, h, planes, r);
+    }
+    const int segs = (h + kColSegment - 1) / kColSegment;
+    const size_t jobs = size_t(planes) * segs * w;
+    const int threads = 256;
+    box_cols_segments<<<unsigned((jobs + threads - 1) / threads), threads, 0, s>>>(tmp, out, w, h, planes, r);
+    return cudaGetLastError();
 }
 
 }  // namespace
+
+int filter_launches(int width, int radius) {
+    if (radius == 0) return 1;
+    return width <= kRowPrefixMaxWidth ? 6 : 7;
+}
 
 size_t filter_scratch_doubles(int width, int height, int layers, int smooth) {
     const size_t n = size_t(width) * height;
@@ -167,10 +286,11 @@ cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s) {
     if (grid > 148 * 32) grid = 148 * 32;
     const int identity = a.radius == 0;
     if (!identity) {
-        pack_planes<<<grid, threads, 0, s>>>(a.image, a.first, planes, n, L, channels);
-        box(planes, tmp, means, w, h, packed, a.radius, s);
+        cudaError_t e = box(planes, a.image, a.first, L, channels, tmp, means, w, h, packed, a.radius, s);
+        if (e != cudaSuccess) return e;
         coefficients<<<grid, threads, 0, s>>>(means, coef, n, channels, a.eps);
-        box(coef, planes, mcoef, w, h, ncoef, a.radius, s);
+        e = box(coef, nullptr, nullptr, L, channels, planes, mcoef, w, h, ncoef, a.radius, s);
+        if (e != cudaSuccess) return e;
     }
     finish_targets<<<grid, threads, 0, s>>>(a.image, a.first, mcoef, a.targets, a.status, n, L, channels, a.smooth,
                                             a.plus, identity);

@@ -94,6 +94,13 @@ enum : int { kTriple = 16 };
 // start, start-0 seed) follow the history in the lane's global array, which
 // shrinks the shared-memory slice.
 enum : int { kColdGlobal = 32 };
+// kBookRolled (with kVectorsShared, kRolled and the global history): the
+// trial point and the trial gradient live only in the lane's slice (the
+// rolled evaluation's slots), so every per-layer loop of the bookkeeping
+// runs rolled: one copy of each loop body instead of L, a smaller
+// instruction footprint and fewer registers, the same operations in the same
+// order.
+enum : int { kBookRolled = 64 };
 constexpr int history_of(int storage) { return storage & 3; }
 
 // The lanes of one pixel. G = 4 (a quad, lanes 0..2 colour channels, lane 3
@@ -235,6 +242,13 @@ template <class T, int L, int BASE> struct History<T, L, kHistGlobal, BASE> {
         }
         next = next + 1 == kHistory ? 0 : next + 1;
     }
+    // The same one element at a time (rolled loops), then advance().
+    __device__ __forceinline__ void push_elem(int l, T sv, T yv) {
+        T* p = base + size_t(next * 2 * L) * lanes;
+        p[size_t(2 * l) * lanes] = sv;
+        p[size_t(2 * l + 1) * lanes] = yv;
+    }
+    __device__ __forceinline__ void advance() { next = next + 1 == kHistory ? 0 : next + 1; }
     __device__ __forceinline__ void reset() { next = 0; }
 };
 
@@ -252,7 +266,9 @@ template <class T, int L, int S> struct LaneSlice {
     // alphas, composite alpha and colour, trial gradient) in the slice.
     static constexpr bool kRolledEval = (S & kRolled) != 0;
     static constexpr int kScratch = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
-    static constexpr int kValues = kScratch + (kRolledEval ? 5 * L : 0);
+    // kBookRolled with three lanes: the pinned alphas' gradient at x.
+    static constexpr int kGa3 = kScratch + (kRolledEval ? 5 * L : 0);
+    static constexpr int kValues = kGa3 + (((S & kBookRolled) && (S & kTriple)) ? L : 0);
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
     }
@@ -269,12 +285,31 @@ enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart,
 // BATCH: pixels of many images (one layer-count group); the quad's layer
 // models are staged in the shared-memory slot that `m` refers to.
 template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSolver {
-    static constexpr int R = REFINE ? L : 1;   // residual rows owned by the alpha lane
+    // Residual rows of a lane: the alpha lane of a refinement owns the L rows
+    // of the pinned alphas; a colour lane owns one (three-lane groups have
+    // colour lanes only). RA: the pinned alphas a lane keeps.
+    static constexpr int R = (REFINE && (S & kTriple) == 0) ? L : 1;
+    static constexpr int RA = REFINE ? L : 1;
     static constexpr int kLanes = (S & kTriple) ? 3 : 4;   // lanes per pixel
     static_assert(kLanes == 4 || (REFINE && !BATCH), "three-lane groups serve the refinement only");
     using Slice = LaneSlice<T, L, S>;
     static constexpr int HS = history_of(S);
     static constexpr bool VS = (S & kVectorsShared) != 0;
+    static constexpr bool BR = (S & kBookRolled) != 0;
+    static_assert(!BR || (VS && (S & kRolled) && HS == kHistGlobal && (!REFINE || kLanes == 3)),
+                  "rolled bookkeeping: x, g, d and the evaluation in the slice, global history, no alpha lane with "
+                  "pinned alphas");
+    // Unroll factors of the per-layer bookkeeping loops: kU for loops over
+    // registers and shared memory (rolled with BR); kUC for loops over the cold
+    // values, which stay unrolled when they live in global memory so that
+    // their loads issue together.
+    static constexpr int kU = BR ? 1 : L;
+    static constexpr int kUC = (BR && (S & kColdGlobal) == 0) ? 1 : L;
+    // The two-loop recursion's per-layer loops over the global history: rolled
+    // in the three-lane refinement (measured faster: 102.5 against 106.5 ms on
+    // the 1024x1024 five-layer image), unrolled in the first pass (145 against
+    // 166 ms: its history loads then issue together).
+    static constexpr int kUT = (BR && kLanes == 3) ? 1 : L;
     const Models<T>* models_;
     const SolverControls& ctl;
     const SolveArgs& a;
@@ -289,15 +324,15 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     int pixel = 0, gidx = 0;   // pixel index within its image, queue index
     int job_id = -1;
     T target, bgq;
-    T ahat[R];           // alpha lane, refinement: filtered alpha targets (pinned alphas)
+    T ahat[RA];          // refinement: filtered alpha targets (pinned alphas)
 
     // Method state (this lane's slice).
     mutable T xr_[VS ? 1 : L], gr_[VS ? 1 : L], dr_[VS ? 1 : L];   // x, g, d in registers (!VS)
-    T tr[L], ng[L];
+    mutable T tr_[BR ? 1 : L], ng_[BR ? 1 : L];   // trial point and gradient in registers (!BR)
     T lam[R], res[R], resx[R];   // multipliers, residual of the last evaluation, residual at x
     // G = 3: every lane's copy of the (pinned) alphas' gradient at x and at the
     // trial point; they enter only y.y of the curvature pairs.
-    T ga3[kLanes == 3 ? L : 1], na3[kLanes == 3 ? L : 1];
+    mutable T ga3_[(kLanes == 3 && !BR) ? L : 1], na3_[(kLanes == 3 && !BR) ? L : 1];
     History<T, L, HS, Slice::kHist> hist;
 
     // Per-quad scalars (uniform within the quad).
@@ -340,6 +375,20 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             return Slice::value(k);
         }
     }
+    // The trial point, the trial gradient and (G = 3) the pinned alphas'
+    // gradient at the trial point and at x: registers, or the slice (BR).
+    __device__ __forceinline__ T& TRv(int l) const {
+        if constexpr (BR) return Slice::value(Slice::kScratch + l); else return tr_[l];
+    }
+    __device__ __forceinline__ T& NGv(int l) const {
+        if constexpr (BR) return Slice::value(Slice::kScratch + 4 * L + l); else return ng_[l];
+    }
+    __device__ __forceinline__ T& NA3(int l) const {
+        if constexpr (BR) return Slice::value(Slice::kScratch + L + l); else return na3_[l];
+    }
+    __device__ __forceinline__ T& GA3(int l) const {
+        if constexpr (BR) return Slice::value(Slice::kGa3 + l); else return ga3_[l];
+    }
     __device__ __forceinline__ T& best(int l) const { return cold(l); }
     __device__ __forceinline__ T& ox(int l) const { return cold(L + l); }
     __device__ __forceinline__ T& init(int l) const { return cold(2 * L + l); }
@@ -366,12 +415,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 
     // ------------------------------------------------------------ bounds --
     __device__ __forceinline__ T lo(int l) const {
-        if (colour) return (REFINE && smooth && l == 0) ? bgq : T(0);
+        if (kLanes == 3 || colour) return (REFINE && smooth && l == 0) ? bgq : T(0);
         if (opaque && l == 0) return T(1);
         return REFINE ? ahat[REFINE ? l : 0] : T(0);
     }
     __device__ __forceinline__ T hi(int l) const {
-        if (colour) return (REFINE && smooth && l == 0) ? bgq : T(1);
+        if (kLanes == 3 || colour) return (REFINE && smooth && l == 0) ? bgq : T(1);
         if (opaque && l == 0) return T(1);
         return REFINE ? ahat[REFINE ? l : 0] : T(1);
     }
@@ -450,7 +499,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         } else if (REFINE) {
 #pragma unroll
             for (int l = 0; l < R; ++l) {
-                res[l] = tr[l] - ahat[l];
+                res[l] = TRv(l) - ahat[l];
                 terms += madd(T(0.5) * rho * res[l], res[l], -(lam[l] * res[l]));
                 norm = madd(res[l], res[l], norm);
             }
@@ -471,8 +520,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                  (!feasible && best_norm >= tol2 && norm < best_norm))) {
                 have_best = true; best_norm = norm; best_energy = energy;
                 best_moved = true;
-#pragma unroll
-                for (int l = 0; l < L; ++l) best(l) = tr[l];
+#pragma unroll kUC
+                for (int l = 0; l < L; ++l) best(l) = TRv(l);
             }
         }
         return value;
@@ -485,16 +534,16 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const Models<T>& m = models();
         T al[L], A[L], pc[L];
 #pragma unroll
-        for (int l = 0; l < L; ++l) al[l] = alpha_at(tr[l], l);
+        for (int l = 0; l < L; ++l) al[l] = alpha_at(TRv(l), l);
         A[0] = al[0];
-        pc[0] = tr[0];
+        pc[0] = TRv(0);
 #pragma unroll
         for (int l = 1; l < L; ++l) {
             const T av = al[l], dd = A[l - 1];
             // X a d + Y a (1 - d) + Z d (1 - a), and the colour the same way.
             const T Al = madd(T(m.Z[l]) * dd, T(1) - av, madd(T(m.X[l]) * av, dd, T(m.Y[l]) * av * (T(1) - dd)));
             A[l] = Al;
-            const T s = tr[l], c = pc[l - 1];
+            const T s = TRv(l), c = pc[l - 1];
             const T pre = madd(T(m.Z[l]) * dd * (T(1) - av), c,
                                madd(blend(m, l, s, c) * av, dd, T(m.Y[l]) * av * (T(1) - dd) * s));
             pc[l] = Al > T(1e-12) ? qdiv(pre, Al) : pre;
@@ -502,7 +551,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         T energy = T(0), asum = T(0);
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const T mine = colour ? tr[l] - mean_of(m, l) : T(0);
+            const T mine = colour ? TRv(l) - mean_of(m, l) : T(0);
             const T d0 = Q.from(mine, 0), d1 = Q.from(mine, 1), d2 = Q.from(mine, 2);
             const T* P = m.prec[l];
             const T v0 = madd(P[2], d2, madd(P[0], d0, P[1] * d1));
@@ -516,11 +565,11 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     const T vq = sel3(Q.q, v0, v1, v2);
                     const T tq = madd(sel3(Q.q, P[6], P[7], P[8]), d2,
                                       madd(sel3(Q.q, P[0], P[1], P[2]), d0, sel3(Q.q, P[3], P[4], P[5]) * d1));
-                    ng[l] = al[l] * (vq + tq);
+                    NGv(l) = al[l] * (vq + tq);
                 } else {
-                    ng[l] = D + (REFINE ? T(0) : T(0.01));
+                    NGv(l) = D + (REFINE ? T(0) : T(0.01));
                 }
-                if constexpr (kLanes == 3) na3[l] = D;
+                if constexpr (kLanes == 3) NA3(l) = D;
             }
         }
         if (!REFINE) energy += T(0.01) * asum;
@@ -530,7 +579,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             T adj3 = (!colour && !REFINE) ? rho * res[0] - lam[0] : T(0);
             if (REFINE && !colour)
 #pragma unroll
-                for (int l = 0; l < R; ++l) ng[l] += rho * res[l] - lam[l];
+                for (int l = 0; l < R; ++l) NGv(l) += rho * res[l] - lam[l];
 #pragma unroll
             for (int l = L - 1; l > 0; --l) {
                 const T av = al[l], dd = A[l - 1], Al = A[l];
@@ -543,7 +592,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     // FP32: the colour channel terms on all four lanes without
                     // a branch (lane 3 would idle through them anyway; its
                     // values are replaced by the alpha chain's terms below).
-                    const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
+                    const T s = TRv(l), c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);
                     const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
@@ -560,10 +609,10 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     } else {
                         ga = v * pa; gp = v * pd; gs = v * ds; ad = v * dc;
                     }
-                    if (colour) { ng[l] += gs; adj = ad; }
+                    if (colour) { NGv(l) += gs; adj = ad; }
                     else { ga = adj3 * da; gp = adj3 * db; }
                 } else if (colour) {
-                    const T s = tr[l], c = pc[l - 1], out = pc[l], v = adj;
+                    const T s = TRv(l), c = pc[l - 1], out = pc[l], v = adj;
                     T fv, fs, fd;
                     blend3(m, l, s, c, fv, fs, fd);
                     const T ds = madd(av * dd, fs, Y * av * (T(1) - dd));
@@ -573,11 +622,11 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                     if (big) {
                         ga = v * ((pa - out * da) / Al);
                         gp = v * ((pd - out * db) / Al);
-                        ng[l] += v * (ds / Al);
+                        NGv(l) += v * (ds / Al);
                         adj = v * (dc / Al);
                     } else {
                         ga = v * pa; gp = v * pd;
-                        ng[l] += v * ds;
+                        NGv(l) += v * ds;
                         adj = v * dc;
                     }
                 } else {
@@ -586,13 +635,13 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 }
                 if constexpr (kLanes == 4) {
                     Q.sum2(ga, gp);
-                    if (!colour) { ng[l] += ga; adj3 = gp; }
+                    if (!colour) { NGv(l) += ga; adj3 = gp; }
                 } else {
-                    alpha_chain(l, da, db, ga, gp, adj3, na3[l]);
+                    alpha_chain(l, da, db, ga, gp, adj3, NA3(l));
                 }
             }
-            ng[0] += colour ? adj : adj3;
-            if constexpr (kLanes == 3) na3[0] += adj3;
+            NGv(0) += colour ? adj : adj3;
+            if constexpr (kLanes == 3) NA3(0) += adj3;
         }
         return value;
     }
@@ -617,12 +666,12 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         auto PC = [sc](int l) -> T& { return sc[(3 * L + l) * kSliceStride]; };
         auto NG = [sc](int l) -> T& { return sc[(4 * L + l) * kSliceStride]; };
         auto NA = [sc](int l) -> T& { return sc[(L + l) * kSliceStride]; };   // G = 3: alpha gradient
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
-            TRc(l) = tr[l];
-            if constexpr (kLanes == 4) ALs(l) = alpha_at(tr[l], l);
+            if constexpr (!BR) TRc(l) = TRv(l);   // (BR: the slot is the trial point)
+            if constexpr (kLanes == 4) ALs(l) = alpha_at(TRc(l), l);
         }
-        T dprev = AL(0), cprev = tr[0];
+        T dprev = AL(0), cprev = TRc(0);
         AA(0) = dprev;
         PC(0) = cprev;
 #pragma unroll 1
@@ -730,19 +779,27 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             }
             NG(0) += colour ? adj : adj3;
             if constexpr (kLanes == 3) NA(0) += adj3;
+            if constexpr (!BR) {
 #pragma unroll
-            for (int l = 0; l < L; ++l) ng[l] = NG(l);
-            if constexpr (kLanes == 3)
+                for (int l = 0; l < L; ++l) NGv(l) = NG(l);
+                if constexpr (kLanes == 3)
 #pragma unroll
-                for (int l = 0; l < L; ++l) na3[l] = NA(l);
+                    for (int l = 0; l < L; ++l) NA3(l) = NA(l);
+            }
         }
         return value;
     }
 
     // ------------------------------------------------------ bookkeeping --
     __device__ __forceinline__ void steepest() {
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) D(l) = fixed_at(l, G(l)) ? T(0) : -G(l);
+    }
+
+    // Layer l is free in this iteration's direction (BR: recomputed from x and
+    // g, which do not change while the direction is formed).
+    __device__ __forceinline__ bool is_free(const bool* freev, int l) const {
+        if constexpr (BR) return !fixed_at(l, G(l)); else return freev[l];
     }
 
     // Two-loop recursion on the current free set; d holds q on entry/exit.
@@ -806,9 +863,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         for (int j = 0; j < valid; ++j) {
             const T* h = hist.row(j);
             T dot = T(0), sy = T(0), ss = T(0), yy = T(0);
-#pragma unroll
+#pragma unroll kUT
             for (int l = 0; l < L; ++l)
-                if (freev[l]) {
+                if (is_free(freev, l)) {
                     const T sa = h[size_t(2 * l) * hs], yb = h[size_t(2 * l + 1) * hs];
                     dot = madd(sa, D(l), dot); sy = madd(sa, yb, sy); ss = madd(sa, sa, ss); yy = madd(yb, yb, yy);
                 }
@@ -816,28 +873,28 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const T r = qdiv(T(1), sy);
             const T inv = (curvature_ok(sy, ss, yy) && finite_(r)) ? r : T(0);
             const T coeff = dot * inv;
-#pragma unroll
+#pragma unroll kUT
             for (int l = 0; l < L; ++l)
-                if (freev[l]) D(l) = madd(-coeff, h[size_t(2 * l + 1) * hs], D(l));
+                if (is_free(freev, l)) D(l) = madd(-coeff, h[size_t(2 * l + 1) * hs], D(l));
             if (!have_scaling && inv > T(0) && yy > T(0)) { scaling = qdiv(sy, yy); have_scaling = true; }
             coeffs[2 * j * kSliceStride] = coeff;
             coeffs[(2 * j + 1) * kSliceStride] = inv;
         }
         scaling = fmax(T(1e-12), fmin(T(1e3), scaling));
-#pragma unroll
+#pragma unroll kUT
         for (int l = 0; l < L; ++l) D(l) *= scaling;
 #pragma unroll 1
         for (int j = valid - 1; j >= 0; --j) {
             const T* h = hist.row(j);
             T dot = T(0);
-#pragma unroll
+#pragma unroll kUT
             for (int l = 0; l < L; ++l)
-                if (freev[l]) dot = madd(h[size_t(2 * l + 1) * hs], D(l), dot);
+                if (is_free(freev, l)) dot = madd(h[size_t(2 * l + 1) * hs], D(l), dot);
             dot = Q.sum(dot);
             const T c = madd(-dot, coeffs[(2 * j + 1) * kSliceStride], coeffs[2 * j * kSliceStride]);
-#pragma unroll
+#pragma unroll kUT
             for (int l = 0; l < L; ++l)
-                if (freev[l]) D(l) = madd(c, h[size_t(2 * l) * hs], D(l));
+                if (is_free(freev, l)) D(l) = madd(c, h[size_t(2 * l) * hs], D(l));
         }
     }
 
@@ -845,7 +902,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ int begin_start() {
         const Models<T>& m = models();
         const int s = start;
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
             T v = init(l);
             if (!REFINE && s == 1) {
@@ -892,8 +949,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
 
     __device__ __forceinline__ int begin_outer() {
         count(4);
-#pragma unroll
-        for (int l = 0; l < L; ++l) { ox(l) = X(l); tr[l] = X(l); }
+#pragma unroll kUC
+        for (int l = 0; l < L; ++l) { ox(l) = X(l); TRv(l) = X(l); }
         phase = kOuterEval;
         best_moved = false;
         return aEval;
@@ -916,7 +973,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         for (int r = 0; r < R; ++r) lam[r] = madd(-rho, resx[r], lam[r]);
         if (norm > T(0.0625) * oldnorm) rho *= T(10);
         T motion = T(0);
-#pragma unroll
+#pragma unroll kUC
         for (int l = 0; l < L; ++l) { const T dl = X(l) - ox(l); motion = madd(dl, dl, motion); }
         motion = Q.sum(motion);
         // A pixel whose last frozen_stop outer steps moved neither x nor the
@@ -951,10 +1008,10 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ int next_trial() {
         if (bt < 32) {
             T sl = T(0), mo = T(0);
-#pragma unroll
+#pragma unroll kU
             for (int l = 0; l < L; ++l) {
-                tr[l] = clampb(l, madd(step, D(l), X(l)));
-                const T delta = tr[l] - X(l);
+                TRv(l) = clampb(l, madd(step, D(l), X(l)));
+                const T delta = TRv(l) - X(l);
                 sl = madd(G(l), delta, sl);
                 mo = madd(delta, delta, mo);
             }
@@ -971,19 +1028,20 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     // direction, first trial.
     __device__ __forceinline__ int begin_iteration() {
         count(2);
-        bool freev[L];
+        bool freev[BR ? 1 : L];
         T pg2 = T(0);
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
-            freev[l] = !fixed_at(l, G(l));
-            D(l) = freev[l] ? G(l) : T(0);
+            const bool fr = !fixed_at(l, G(l));
+            if constexpr (!BR) freev[l] = fr;
+            D(l) = fr ? G(l) : T(0);
             pg2 = madd(D(l), D(l), pg2);
         }
         pg2 = Q.sum(pg2);
         if (pg2 < T(1e-16) || !finite_(f)) return aEndOuter;
         two_loop(freev);
         T descent = T(0);
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
             T v = -D(l);
             const T lv = lo(l), hv = hi(l);
@@ -1001,13 +1059,13 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     // termination test.
     __device__ __forceinline__ int accept() {
         T sy = T(0), ss = T(0), yy = T(0), mm = T(0);
-        T sv[L], yv[L];
-#pragma unroll
+        T sv[BR ? 1 : L], yv[BR ? 1 : L];
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
-            sv[l] = tr[l] - X(l);
-            yv[l] = ng[l] - G(l);
-            sy = madd(sv[l], yv[l], sy); ss = madd(sv[l], sv[l], ss); yy = madd(yv[l], yv[l], yy);
-            if constexpr (kFast || !Slice::kRolledEval) mm = fmax(mm, qdiv(fabs(sv[l]), T(1) + fabs(X(l))));
+            const T svl = TRv(l) - X(l), yvl = NGv(l) - G(l);
+            if constexpr (!BR) { sv[l] = svl; yv[l] = yvl; }
+            sy = madd(svl, yvl, sy); ss = madd(svl, svl, ss); yy = madd(yvl, yvl, yy);
+            if constexpr (kFast || !Slice::kRolledEval) mm = fmax(mm, qdiv(fabs(svl), T(1) + fabs(X(l))));
         }
         if constexpr (!kFast && Slice::kRolledEval) {
             // One copy of the FP64 division: the step from the accepted point
@@ -1023,22 +1081,29 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             // The pinned alphas do not move, but their gradient change counts
             // in y.y (the same on every lane).
             T ya = T(0);
-#pragma unroll
-            for (int l = 0; l < L; ++l) { const T dy = na3[l] - ga3[l]; ya = madd(dy, dy, ya); }
+#pragma unroll kU
+            for (int l = 0; l < L; ++l) { const T dy = NA3(l) - GA3(l); ya = madd(dy, dy, ya); }
             yy += ya;
         }
         mm = Q.max(mm);
         const T r = qdiv(T(1), sy);
         if (curvature_ok(sy, ss, yy) && finite_(r)) {
-            hist.push(sv, yv);
+            if constexpr (BR) {
+                // The pair again, element by element (the same differences).
+#pragma unroll 1
+                for (int l = 0; l < L; ++l) hist.push_elem(l, TRv(l) - X(l), NGv(l) - G(l));
+                hist.advance();
+            } else {
+                hist.push(sv, yv);
+            }
             valid = valid + 1 < kHistory ? valid + 1 : kHistory;
         }
         const T delta = fabs(f - cand), size = T(0.5) * (fabs(f) + fabs(cand));
-#pragma unroll
-        for (int l = 0; l < L; ++l) { X(l) = tr[l]; G(l) = ng[l]; }
+#pragma unroll kU
+        for (int l = 0; l < L; ++l) { X(l) = TRv(l); G(l) = NGv(l); }
         if constexpr (kLanes == 3)
-#pragma unroll
-            for (int l = 0; l < L; ++l) ga3[l] = na3[l];
+#pragma unroll kU
+            for (int l = 0; l < L; ++l) GA3(l) = NA3(l);
 #pragma unroll
         for (int q = 0; q < R; ++q) resx[q] = res[q];
         f = cand;
@@ -1051,11 +1116,11 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     __device__ __forceinline__ int after_evaluation(T value, bool need_grad) {
         if (phase == kOuterEval) {
             f = value;
-#pragma unroll
-            for (int l = 0; l < L; ++l) G(l) = ng[l];
+#pragma unroll kU
+            for (int l = 0; l < L; ++l) G(l) = NGv(l);
             if constexpr (kLanes == 3)
-#pragma unroll
-                for (int l = 0; l < L; ++l) ga3[l] = na3[l];
+#pragma unroll kU
+                for (int l = 0; l < L; ++l) GA3(l) = NA3(l);
 #pragma unroll
             for (int q = 0; q < R; ++q) resx[q] = res[q];
             oldnorm = Q.sum(own_norm(res));
@@ -1086,16 +1151,16 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         target = T(colour ? image()[3 * size_t(i) + Q.q] : 0.0);
         bgq = T((REFINE && smooth && colour) ? a.targets[(size_t(L) + Q.q) * n + i] : 0.0);
 #pragma unroll
-        for (int l = 0; l < R; ++l) {
+        for (int l = 0; l < RA; ++l) {
             double t = REFINE ? a.targets[size_t(l) * n + i] : 0.0;
             if (REFINE && opaque && l == 0) t = 1.0;
             ahat[l] = T(t);
         }
         const float* wp = REFINE ? nullptr : warm();
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
             T v;
-            if (colour) {
+            if (kLanes == 3 || colour) {
                 if (REFINE) v = (smooth && l == 0) ? bgq : T(a.first[(size_t(l) * n + i) * 4 + Q.q]);
                 else v = fmin(T(1), fmax(T(0), mean_of(m, l)));
             } else {
@@ -1124,7 +1189,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         const size_t n = pixels(), i = size_t(pixel);
         double* outp = output();
         double v0 = 0.0;
-#pragma unroll
+#pragma unroll kU
         for (int l = 0; l < L; ++l) {
             double v = double(have_best ? best(l) : init(l));
             if (REFINE && !colour) v = (opaque && l == 0) ? 1.0 : a.targets[size_t(l) * n + i];
@@ -1144,7 +1209,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             const double al = kLanes == 3 ? a.targets[size_t(l) * n + i] : Q.from(s, 3), dd = A;
             const double Al = double(m.X[l]) * al * dd + double(m.Y[l]) * al * (1.0 - dd) +
                               double(m.Z[l]) * dd * (1.0 - al);
-            const double pre = blend_value<double>(m.mode[l], s, c) * al * dd + double(m.Y[l]) * al * (1.0 - dd) * s +
+            const double pre = blend_value_call<double>(m.mode[l], s, c) * al * dd + double(m.Y[l]) * al * (1.0 - dd) * s +
                                double(m.Z[l]) * dd * (1.0 - al) * c;
             c = Al > 1e-12 ? pre / Al : pre;
             A = Al;

@@ -21,7 +21,9 @@ namespace unb {
 // Variant 5 (FP32 and FP64): the refinement with three lanes per pixel (its
 // alphas are pinned, so no alpha lane: 10 pixels per warp), FP32 as 3 and
 // FP64 as 2 otherwise; first passes run variant 3 / 2 for it.
-constexpr int kFp32Variants = 6, kFp64Variants = 6;
+// FP64 variant 6: 3 (first pass) and 5 (refinement) with the bookkeeping's
+// per-layer loops rolled, the trial point and gradient in the slice.
+constexpr int kFp32Variants = 6, kFp64Variants = 7;
 inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant == 4; }
 // Blocks per SM that a global-history array is sized for (the launch clamps
 // its grid to the array).
@@ -81,6 +83,7 @@ struct FilterArgs {
     double* scratch = nullptr;       // filter_scratch_doubles() doubles
 };
 size_t filter_scratch_doubles(int width, int height, int layers, int smooth);
+int filter_launches(int width, int radius);   // kernels one launch_filter call issues
 cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s);
 
 // Fixed scratch of the allocation-free first pass (noalloc.cu): device

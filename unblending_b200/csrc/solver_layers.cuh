@@ -58,6 +58,14 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
         if constexpr (R && !BATCH)
             return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple, 3, BATCH>(m, c, a, threads, sms, s);
         else return go<double, R, kHistGlobal | kVectorsShared | kRolled, 3, BATCH>(m, c, a, threads, sms, s);
+    case 6:   // 3 (first pass) and 5 (refinement) with the bookkeeping rolled over the layers
+        if constexpr (R && !BATCH)
+            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple | kBookRolled, 3, BATCH>(m, c, a, threads,
+                                                                                                       sms, s);
+        else if constexpr (!R)
+            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal | kBookRolled, 4, BATCH>(
+                m, c, a, threads, sms, s);
+        else return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
     }
 }

@@ -244,7 +244,12 @@ int default_fp32_variant(int L, bool refine) { (void)L; return refine ? 5 : 3; }
 // First passes with the cold values in the global array too (variant 3, a
 // smaller shared slice for 4 blocks per SM): re-solve 60.6 -> 53.0 ms, FP64 solve
 // of every pixel 292 -> 248 ms (for the refinement it gains nothing).
-int default_fp64_variant(bool refine) { return refine ? 5 : 3; }
+// The refinement with the bookkeeping rolled over the layers (variant 6; its
+// smaller instruction footprint cut instruction-fetch stalls from 3.6 to 1.4
+// cycles per issue): 106.5 -> 102.5 ms. The first pass keeps variant 3 (its
+// rolled form ran 145 against 139 ms: more instructions, and loads of its
+// global cold values no longer issued together).
+int default_fp64_variant(bool refine) { return refine ? 6 : 3; }
 int fp64_variant(const unblending_solver_options& so, bool refine) {
     return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
 }
@@ -424,7 +429,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         f.targets = targets; f.status = fstatus;
         f.scratch = R.radius > 0 ? c.scratch.get<double>(filter_scratch_doubles(sp.width, sp.height, L, sp.smooth)) : nullptr;
         ck(launch_filter(f, s));
-        t_launches += R.radius > 0 ? 7 : 1;
+        t_launches += filter_launches(sp.width, R.radius);
     }
     ck(cudaEventRecord(c.ev[1], s));
 
