@@ -283,7 +283,7 @@ enum : int { kIdle = 0, kOuterEval = 1, kTrial = 2, kAcceptGrad = 3 };
 enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart, aBeginOuter, aFinish, aFetch };
 
 // BATCH: pixels of many images (one layer-count group); the quad's layer
-// models are staged in the shared-memory slot that `m` refers to.
+// models are those of its current image in the device model table.
 template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSolver {
     // Residual rows of a lane: the alpha lane of a refinement owns the L rows
     // of the pinned alphas; a colour lane owns one (three-lane groups have
@@ -311,6 +311,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
     // 166 ms: its history loads then issue together).
     static constexpr int kUT = (BR && kLanes == 3) ? 1 : L;
     const Models<T>* models_;
+    const Models<T>* batch_models_ = nullptr;   // batched launch: the current image's models
     const SolverControls& ctl;
     const SolveArgs& a;
     Group<kLanes> Q;
@@ -353,13 +354,18 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         itol = T(ctl.inner_tolerance);
         phase = kIdle;
         hist.init(a.history);
+        // Batched: every lane evaluates on every trip, including the lanes of
+        // a quad that has not fetched a pixel yet (or never will, in a batch
+        // smaller than the grid), so the models point at a valid entry from
+        // the start.
+        if constexpr (BATCH) batch_models_ = static_cast<const Models<T>*>(a.models);
     }
 
-    // The layer models: the kernel parameter, or the quad's shared-memory
-    // slot in a batched launch.
+    // The layer models: the kernel parameter, or (batched launch) the
+    // current image's entry of the device model table (read through L1; the
+    // quads of a warp mostly share it).
     __device__ __forceinline__ const Models<T>& models() const {
-        if constexpr (BATCH)
-            return reinterpret_cast<const Models<T>*>(solver_smem + Slice::bytes())[threadIdx.x >> 2];
+        if constexpr (BATCH) return *batch_models_;
         else return *models_;
     }
 
@@ -410,7 +416,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if constexpr (BATCH) return a.jobs[job_id].warm; else return a.warm;
     }
     __device__ __forceinline__ size_t pixels() const {
-        if constexpr (BATCH) return size_t(a.jobs[job_id].n); else return size_t(a.n);
+        if constexpr (BATCH) return job_id < 0 ? size_t(0) : size_t(a.jobs[job_id].n);
+        else return size_t(a.n);
     }
 
     // ------------------------------------------------------------ bounds --
@@ -1261,11 +1268,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
                 if (a.jobs[mid].offset <= int64_t(gidx)) lo = mid; else hi = mid - 1;
             }
             if (lo != job_id) {
-                // Stage this image's layer models in the quad's slot (a typed
-                // copy: the solver reads the fields with their types).
-                __syncwarp(Q.mask);
-                if (Q.q == 0) const_cast<Models<T>&>(models()) = static_cast<const Models<T>*>(a.models)[a.jobs[lo].model];
-                __syncwarp(Q.mask);
+                batch_models_ = static_cast<const Models<T>*>(a.models) + a.jobs[lo].model;
                 job_id = lo;
             }
             i = gidx - int(a.jobs[lo].offset);

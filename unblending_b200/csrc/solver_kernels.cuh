@@ -7,13 +7,10 @@
 namespace unb {
 
 // Dynamic shared memory: every lane's slice (cold values, the L-BFGS
-// history when it is kept there, work counters), then one layer-model slot per quad
-// (BATCH).
+// history when it is kept there, the rolled evaluation's intermediates).
 template <class T, int L, int S, bool BATCH> struct SolveSmem {
     using Slice = LaneSlice<T, L, S>;
-    static size_t bytes(int threads) {
-        return Slice::bytes() + (BATCH ? size_t(threads / 4) * sizeof(Models<T>) : 0);
-    }
+    static size_t bytes(int threads) { (void)threads; return Slice::bytes(); }
 };
 
 // S: storage policy (history place | kVectorsShared); MINB: blocks per SM
