@@ -478,7 +478,7 @@ def solve_roofline(wl, s1, s2, stages, precision):
         grads = s1["fp32_gradients"] + s2["fp32_gradients"]
         ms = stages["unmix_solve"] + stages["refine_solve"]
         peak, kernel = PEAK_FP32_TFLOPS, f"solve_pixels<float,{L},...>"
-        traffic = profile_traffic("solve_pixels_rgb1024_l5.md")
+        traffic = profile_traffic("solve_pixels_fp32_rgb1024_l5.md")
     flops = float((vals - grads) * f_val + grads * f_grad)
     achieved = flops / (ms / 1e3) / 1e12
     return {"bound": precision, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
