@@ -260,10 +260,10 @@ int orc_solve(const orc_layer* layers, const orc_problem* problem, const orc_opt
 
 // The same method in FP32 arithmetic (the oracle templated on float; inputs
 // rounded to float, results widened back): how far a change of precision
-// alone moves the method's results.
+// alone moves the method's results. counters (n*5, or null) as orc_solve's.
 int orc_solve_f32(const orc_layer* layers, const orc_problem* problem, const orc_options* options, size_t n,
                   const double* target, const double* alpha, const double* bg, const double* initial, double* out,
-                  int threads) {
+                  uint32_t* counters, int threads) {
     if (!problem || problem->layers <= 0 || problem->layers > kMaxLayers) return 1;
     const auto models = to_layers(layers, problem->layers);
     const Problem p = to_problem(problem);
@@ -281,9 +281,14 @@ int orc_solve_f32(const orc_layer* layers, const orc_problem* problem, const orc
             }
             for (int l = 0; l < L; ++l) a[l] = alpha ? float(alpha[size_t(L) * i + l]) : 0.0f;
             for (int k = 0; k < N; ++k) x0[k] = float(initial[size_t(N) * i + k]);
-            s.target = t3; s.alpha = a; s.bg = g3; s.counters = nullptr;
+            Counters c;
+            s.target = t3; s.alpha = a; s.bg = g3; s.counters = &c;
             s.run(x0, x1);
             for (int k = 0; k < N; ++k) out[size_t(N) * i + k] = double(x1[k]);
+            if (counters) {
+                uint32_t* o = counters + 5 * i;
+                o[0] = c.values; o[1] = c.gradients; o[2] = c.iterations; o[3] = c.backtracks; o[4] = c.outer;
+            }
         }
     });
     return 0;
