@@ -109,6 +109,8 @@ def parse():
     p.add_argument("--no-fp32", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the rgb256_l3 / rgb4096_l6 keys")
     p.add_argument("--fp64-variant", type=int, default=-1, help="FP64 kernel variant of the default solve (-1: tuned)")
+    p.add_argument("--pixel-order", type=int, default=1, choices=[0, 1],
+                   help="work-queue order of the default solve: 1 grouped by colour (default), 0 image order")
     return p.parse_args()
 
 
@@ -538,7 +540,7 @@ def b200_arm(args):
     D = Decomposition(U, torch, wl, stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     # UNBLENDING_SOLVER_OPTIONS_INIT with the workload's radius.
-    default = U.solver_options(radius=radius, fp64_variant=args.fp64_variant)
+    default = U.solver_options(radius=radius, fp64_variant=args.fp64_variant, pixel_order=args.pixel_order)
 
     sampler = ClockSampler(local)
     if world > 1:

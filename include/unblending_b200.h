@@ -66,11 +66,16 @@ typedef struct unblending_solver_options {
                                    stop a pixel after this many consecutive outer steps that moved neither its
                                    point nor its best point (default 4; 0 = run to the outer cap, the
                                    reference's schedule; results equal on every tested image) */
+    int32_t pixel_order;        /* order in which a solve hands out the pixels it solves: 1 (default) grouped by
+                                   colour (a Morton order of the quantized RGB), so the pixels that one warp solves
+                                   together take similar paths through the method; 0 image order. Results do not
+                                   depend on it. A caller built against the previous layout, whose struct_size
+                                   ends before this field, gets the default. */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
     { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP64, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, \
-      NULL, -1, 9, 3, 4 }
+      NULL, -1, 9, 3, 4, 1 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

@@ -128,10 +128,31 @@ def test_solver_option_validation(small):
     for bad in [dict(precision=3), dict(starts=0), dict(starts=4), dict(epsilon=0.0), dict(inner=0),
                 dict(threads_per_block=48), dict(resolve_misses=2), dict(fp32_outer=-1), dict(gradient_quorum=9),
                 dict(gradient_quorum=-1), dict(frozen_stop=-1), dict(kernel_variant=6),
-                dict(fp64_variant=7)]:
+                dict(fp64_variant=7), dict(pixel_order=2), dict(pixel_order=-1)]:
         so = U.solver_options(**bad)
         with pytest.raises(ValueError):
             U.unmix_ex(small.image, small.layers, solver=so)
+
+
+def test_solver_options_of_the_previous_layout_are_accepted(small):
+    # A caller built before pixel_order existed passes a struct_size that ends
+    # at that field: the call reads none of it (the garbage value below would
+    # be rejected) and takes the default. One word shorter is rejected.
+    import ctypes as C
+    import torch
+    cuda_present = torch.cuda.is_available()
+    short = U.SolverOptions.pixel_order.offset
+    so = U.solver_options(pixel_order=7)
+    so.struct_size = short
+    if cuda_present:
+        U.unmix_ex(small.image, small.layers, solver=so)
+    else:
+        with pytest.raises(U.ExecutionError):   # validation passed; no device to run on
+            U.unmix_ex(small.image, small.layers, solver=so)
+    so.struct_size = short - 4
+    with pytest.raises(ValueError):
+        U.unmix_ex(small.image, small.layers, solver=so)
+    assert C.sizeof(U.SolverOptions) > short
 
 
 def test_noalloc_rejects_images_beyond_its_scratch_before_any_device_work():

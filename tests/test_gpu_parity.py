@@ -308,6 +308,37 @@ def test_warp_scheduling_quorum_leaves_results_unchanged(cuda, precision):
             assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_colour_ordered_queue_leaves_results_unchanged(cuda, precision):
+    """The solves hand out their pixels grouped by colour (pixel_order 1, the
+    default) or in image order (0); each pixel's solve reads only its own
+    inputs, so both passes, their statuses and counters are bit-identical,
+    and so are the row-range entry points, whose order covers only their rows."""
+    wl = syn.generate(72, 56, [0, 1, 2, 3, 6], (4.0, 16.0), seed=91)
+    outs = []
+    for order in (1, 0):
+        so = solver(cuda, precision, radius=3, pixel_order=order)
+        first, st1, c1, _ = cuda.unmix_ex(wl.image, wl.layers, solver=so, with_counters=True)
+        final, st2, c2, _ = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so, with_counters=True)
+        outs.append((first, st1, c1, final, st2, c2))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    import torch
+    n, L = wl.pixels, len(wl.layers)
+    d_img = torch.from_numpy(wl.image.reshape(-1)).cuda()
+    bands = []
+    for order in (1, 0):
+        so = solver(cuda, precision, radius=3, pixel_order=order)
+        d_first = torch.full((4 * L * n,), float("nan"), dtype=torch.float64, device="cuda")
+        for r0, r1 in ((0, 13), (13, 40), (40, 56)):
+            cuda.unmix_device_rows(wl.width, wl.height, d_img.data_ptr(), wl.layers, d_first.data_ptr(), r0, r1,
+                                   solver=so)
+        torch.cuda.synchronize()
+        bands.append(d_first.cpu().numpy())
+    assert np.array_equal(bands[0], bands[1])
+    assert np.array_equal(bands[0].reshape(outs[0][0].shape), outs[0][0])
+
+
 FROZEN_CASES = [
     ("rgb1024_l5", 160, 128, None),
     ("rgb4096_l6", 160, 128, None),

@@ -33,6 +33,7 @@ UNITS = [
     ("solver_launch.cu", []),
     ("filter.cu", ["--fmad=false"]),
     ("noalloc.cu", []),
+    ("order.cu", []),
     ("mlp.cu", []),
     ("mlp_data.cu", []),
     ("pixels.cpp", ["-I" + os.path.join(ROOT, "include")]),

@@ -117,6 +117,9 @@ struct SolveArgs {
     // Without a list: the launch solves pixels [first_pixel, first_pixel +
     // pixel_count) of the image (pixel_count < 0: all n).
     int first_pixel = 0, pixel_count = -1;
+    // Without a list: optional queue order, the pixel index of each queue
+    // index (a permutation of the pixels the launch solves); null = in order.
+    const int32_t* order = nullptr;
 };
 
 }  // namespace unb

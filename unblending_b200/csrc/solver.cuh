@@ -1258,7 +1258,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if (Q.q == 0) job = int(atomicAdd(a.queue, 1u));
         job = Q.from(job, 0);
         if (job >= total) { phase = kIdle; live = false; return aEval; }
-        gidx = a.list ? a.list[job] : a.first_pixel + job;
+        gidx = a.list ? a.list[job] : (a.order ? a.order[job] : a.first_pixel + job);
         int i = gidx;
         if constexpr (BATCH) {
             // The image owning queue index gidx: last job with offset <= gidx.

@@ -86,6 +86,13 @@ size_t filter_scratch_doubles(int width, int height, int layers, int smooth);
 int filter_launches(int width, int radius);   // kernels one launch_filter call issues
 cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s);
 
+// Work-queue order of a solve launch (order.cu): the pixels [first, first +
+// count) of an image, grouped by colour, into order[0, count); `cells` is
+// scratch of order_cells(count) words.
+size_t order_cells(int count);
+cudaError_t launch_pixel_order(const double* image, int first, int count, uint32_t* cells, int32_t* order, int sms,
+                               cudaStream_t s);
+
 // Fixed scratch of the allocation-free first pass (noalloc.cu): device
 // address on the current device (resolved on the first call per device),
 // its size, and the largest image it serves.

@@ -90,6 +90,7 @@ struct Context {
     cudaEvent_t ev[6] = {};
     std::mutex mutex;
     Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters, history;
+    Buffer order, order_cells;               // work-queue order of a pass (order.cu) and its counting-sort cells
     Buffer warm, mlp_w, mlp_b;               // warm-start network on the device
     std::vector<float> mlp_uploaded;         // parameters currently in mlp_w / mlp_b
     // Concurrent branches of a batched pass (one per layer-count group) and
@@ -214,8 +215,10 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
     const unblending_solver_options defaults = UNBLENDING_SOLVER_OPTIONS_INIT;
     out = defaults;
     if (!in) return UNBLENDING_OK;
-    if (in->struct_size < sizeof(unblending_solver_options)) return UNBLENDING_INVALID_ARGUMENT;
-    out = *in;
+    // Callers built before pixel_order was added pass the shorter layout; the
+    // fields they do not have keep their defaults.
+    if (in->struct_size < offsetof(unblending_solver_options, pixel_order)) return UNBLENDING_INVALID_ARGUMENT;
+    std::memcpy(&out, in, std::min<size_t>(in->struct_size, sizeof(unblending_solver_options)));
     out.struct_size = sizeof(unblending_solver_options);
     if ((out.precision != UNBLENDING_PRECISION_FP32 && out.precision != UNBLENDING_PRECISION_FP64) ||
         out.starts < 1 || out.starts > 3 || !(out.epsilon > 0) || !std::isfinite(out.epsilon) || out.inner < 1 ||
@@ -225,7 +228,7 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
                                         out.threads_per_block > 128)) ||
         out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
         out.fp64_variant >= kFp64Variants || out.fp32_outer < 0 || out.gradient_quorum < 0 ||
-        out.gradient_quorum > 8 || out.frozen_stop < 0)
+        out.gradient_quorum > 8 || out.frozen_stop < 0 || (out.pixel_order != 0 && out.pixel_order != 1))
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -450,6 +453,15 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     a.miss_list = c.list_a.get<int32_t>(n);
     a.miss_count = counts + 0;
     a.tally = R.tally;
+    if (so.pixel_order) {
+        // The solve hands out its pixels grouped by colour (order.cu).
+        const int count = io.pixel_count >= 0 ? io.pixel_count : int(n);
+        int32_t* order = c.order.get<int32_t>(size_t(count));
+        uint32_t* cells = c.order_cells.get<uint32_t>(order_cells(count));
+        ck(launch_pixel_order(io.image, io.first_pixel, count, cells, order, c.sms, s));
+        t_launches += 4;
+        a.order = order;
+    }
     if (!refine && so.warm_start) {
         // Learned start point for every pixel, then the solve from it.
         const MlpDevice dev = upload_model(c, *so.warm_start, s);
