@@ -25,14 +25,38 @@ namespace {
 
 constexpr int kMinOrderBits = 4, kMaxOrderBits = 7;
 
-// Cell of pixel i: the bits of the three quantized channels interleaved
+// The pixels being ordered: queue index k is pixel first + k of `image`,
+// or (a batched group) queue index k of `jobs`, in the image whose offset is
+// the last one <= k.
+struct OrderSource {
+    const double* image;
+    int first;
+    const BatchJob* jobs;
+    int job_count;
+    // The RGB of queue index k, and the value the order stores for it.
+    __device__ __forceinline__ const double* rgb(int k, int32_t& value) const {
+        if (!jobs) {
+            value = first + k;
+            return image + 3 * size_t(value);
+        }
+        int lo = 0, hi = job_count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].offset <= int64_t(k)) lo = mid; else hi = mid - 1;
+        }
+        value = k;
+        return jobs[lo].image + 3 * size_t(int64_t(k) - jobs[lo].offset);
+    }
+};
+
+// Cell of a pixel: the bits of the three quantized channels interleaved
 // (bit b of channel c at bit 3b + c). NaN and negative values fall in level 0,
 // values >= 1 in the top level.
-__device__ __forceinline__ uint32_t colour_cell(const double* image, size_t i, int bits) {
+__device__ __forceinline__ uint32_t colour_cell(const double* rgb, int bits) {
     uint32_t key = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double v = image[3 * i + c];
+        const double v = rgb[c];
         const uint32_t q = v >= 0.0 ? (v < 1.0 ? uint32_t(v * double(1 << bits)) : (1u << bits) - 1u) : 0u;
 #pragma unroll
         for (int b = 0; b < kMaxOrderBits; ++b)
@@ -41,10 +65,11 @@ __device__ __forceinline__ uint32_t colour_cell(const double* image, size_t i, i
     return key;
 }
 
-__global__ void order_count(const double* __restrict__ image, int first, int count, int bits,
-                            uint32_t* __restrict__ cells) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x)
-        atomicAdd(&cells[colour_cell(image, size_t(first) + size_t(k), bits)], 1u);
+__global__ void order_count(const OrderSource src, int count, int bits, uint32_t* __restrict__ cells) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        int32_t value;
+        atomicAdd(&cells[colour_cell(src.rgb(k, value), bits)], 1u);
+    }
 }
 
 // Exclusive prefix sum of the cell counts, in place, in chunks of
@@ -111,11 +136,12 @@ __global__ void __launch_bounds__(kScanThreads) order_chunk_scan(uint32_t* __res
     }
 }
 
-__global__ void order_scatter(const double* __restrict__ image, int first, int count, int bits,
-                              uint32_t* __restrict__ cells, int32_t* __restrict__ order) {
+__global__ void order_scatter(const OrderSource src, int count, int bits, uint32_t* __restrict__ cells,
+                              int32_t* __restrict__ order) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        const size_t i = size_t(first) + size_t(k);
-        order[atomicAdd(&cells[colour_cell(image, i, bits)], 1u)] = int32_t(i);
+        int32_t value;
+        const double* rgb = src.rgb(k, value);
+        order[atomicAdd(&cells[colour_cell(rgb, bits)], 1u)] = value;
     }
 }
 
@@ -135,8 +161,8 @@ size_t order_cells(int count) {
     return cells + cells / kScanChunk;
 }
 
-cudaError_t launch_pixel_order(const double* image, int first, int count, uint32_t* cells, int32_t* order, int sms,
-                               cudaStream_t s) {
+namespace {
+cudaError_t launch_order(const OrderSource& src, int count, uint32_t* cells, int32_t* order, int sms, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const int bits = order_bits(count);
     const int cell_count = 1 << (3 * bits);
@@ -146,11 +172,22 @@ cudaError_t launch_pixel_order(const double* image, int first, int count, uint32
     const int blocks = std::min((count + threads - 1) / threads, 8 * sms);
     const int chunks = cell_count / kScanChunk;
     uint32_t* sums = cells + cell_count;
-    order_count<<<blocks, threads, 0, s>>>(image, first, count, bits, cells);
+    order_count<<<blocks, threads, 0, s>>>(src, count, bits, cells);
     order_chunk_sums<<<chunks, kScanThreads, 0, s>>>(cells, sums);
     order_chunk_scan<<<chunks, kScanThreads, 0, s>>>(cells, sums);
-    order_scatter<<<blocks, threads, 0, s>>>(image, first, count, bits, cells, order);
+    order_scatter<<<blocks, threads, 0, s>>>(src, count, bits, cells, order);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_pixel_order(const double* image, int first, int count, uint32_t* cells, int32_t* order, int sms,
+                               cudaStream_t s) {
+    return launch_order(OrderSource{image, first, nullptr, 0}, count, cells, order, sms, s);
+}
+
+cudaError_t launch_group_order(const BatchJob* jobs, int job_count, int total, uint32_t* cells, int32_t* order,
+                               int sms, cudaStream_t s) {
+    return launch_order(OrderSource{nullptr, 0, jobs, job_count}, total, cells, order, sms, s);
 }
 
 }  // namespace unb

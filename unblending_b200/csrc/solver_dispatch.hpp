@@ -92,6 +92,10 @@ cudaError_t launch_filter(const FilterArgs& a, cudaStream_t s);
 size_t order_cells(int count);
 cudaError_t launch_pixel_order(const double* image, int first, int count, uint32_t* cells, int32_t* order, int sms,
                                cudaStream_t s);
+// The same over the `total` queue indices of a batched group (order[k] is a
+// queue index of the group; the pixels' colours are read through `jobs`).
+cudaError_t launch_group_order(const BatchJob* jobs, int job_count, int total, uint32_t* cells, int32_t* order,
+                               int sms, cudaStream_t s);
 
 // Fixed scratch of the allocation-free first pass (noalloc.cu): device
 // address on the current device (resolved on the first call per device),

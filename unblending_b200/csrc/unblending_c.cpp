@@ -820,6 +820,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
     put(&so.fp64_variant, sizeof(so.fp64_variant)); put(&so.fp32_outer, sizeof(so.fp32_outer));
     put(&so.gradient_quorum, sizeof(so.gradient_quorum));
     put(&so.frozen_stop, sizeof(so.frozen_stop));
+    put(&so.pixel_order, sizeof(so.pixel_order));
     for (int k = 0; k < count; ++k) {
         const auto& J = jobs[k];
         put(&J.width, sizeof(J.width)); put(&J.height, sizeof(J.height));
@@ -848,6 +849,9 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 std::vector<std::pair<int, float*>> infer;   // job, warm slice
                 MlpDevice net;
                 int variant = 0, threads = 128;
+                int64_t total = 0;
+                int32_t* order = nullptr;   // colour order of the group's queue (pixel_order)
+                uint32_t* order_cells = nullptr;
             };
             std::vector<Group> gs;
             for (auto& [L, members] : groups) {
@@ -861,6 +865,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 float* warm = nullptr;
                 int64_t total = 0;
                 for (int k : members) total += int64_t(specs[k].pixels);
+                G.total = total;
                 if (net) warm = plan->alloc<float>(size_t(total) * 4 * L);
                 for (int k : members) {
                     const auto& J = jobs[k];
@@ -903,14 +908,20 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                 G.queues = plan->alloc<uint32_t>(8);
                 G.counts = reinterpret_cast<int32_t*>(G.queues + 4);
                 int32_t* lists = plan->alloc<int32_t>(2 * size_t(total));
+                if (so.pixel_order) {
+                    G.order = plan->alloc<int32_t>(size_t(total));
+                    G.order_cells = plan->alloc<uint32_t>(order_cells(int(total)));
+                }
                 SolveArgs& a = G.fp;
                 a.n = int(total);
                 a.jobs = d_table; a.job_count = int(table.size());
                 a.opaque = specs[members[0]].opaque; a.smooth = 0;
                 a.queue = G.queues;
                 a.miss_list = lists; a.miss_count = G.counts + 0;
+                a.order = G.order;
                 SolveArgs& b = G.re;
                 b = a;
+                b.order = nullptr;
                 b.jobs = d_table + table.size();
                 b.models = d_m64;
                 b.list = lists; b.list_count = G.counts + 0;
@@ -922,6 +933,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     // with the same result), its misses the FP64 re-solve.
                     SolveArgs& w = G.mid;
                     w = a;
+                    w.order = nullptr;
                     w.jobs = d_table + table.size();
                     w.models = d_m32;
                     w.list = lists; w.list_count = G.counts + 0;
@@ -985,9 +997,11 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
             // branch: the groups' persistent launches run back to back on the
             // GPU, the next group's blocks filling the SMs that the previous
             // group's tail frees. (One kernel over all layer counts was built
-            // and measured: its single register allocation over every layer
-            // count's solver spilled 0.6-1.6 KB of stack per thread, against
-            // at most 64 bytes for the per-count kernels.)
+            // and measured twice: with every solver inlined, its single
+            // register allocation spilled 0.6-1.6 KB of stack per thread; with
+            // each count's solver out of line, it ran 4.45 against 6.52 Mpx/s
+            // on a 64-image batch, its one shared-memory size set by the
+            // largest layer count holding every group's occupancy down.)
             if (!c.fork) {
                 ck(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
                 for (int q = 0; q < kMaxLayers; ++q) {
@@ -1005,6 +1019,12 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
                     cudaStream_t s = c.branch[gi];   // this group's branch (shadows the call's stream)
                     ck(cudaStreamWaitEvent(s, c.fork, 0));
                     ck(cudaMemsetAsync(G.queues, 0, 8 * sizeof(uint32_t), s));
+                    if (G.order) {
+                        // The group's queue grouped by colour (order.cu).
+                        ck(launch_group_order(G.fp.jobs, G.fp.job_count, int(G.total), G.order_cells, G.order, c.sms,
+                                              s));
+                        launches += 4;
+                    }
                     for (auto& [k, w] : G.infer) {
                         ck(launch_mlp_infer(G.net, jobs[k].image, jobs[k].width, jobs[k].height, G.L, w, G.counts + 3,
                                             c.sms, s));
