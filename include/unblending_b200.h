@@ -54,7 +54,11 @@ typedef struct unblending_solver_options {
                                    uncapped registers, 1 capped for 2 blocks per SM; 2 history in global memory,
                                    x/g/d in shared memory, evaluation rolled, 3 blocks per SM; 3 as 2 with the
                                    start and bounds in global memory, 4 blocks per SM; 4/5 as 3/2 with three
-                                   lanes per pixel where the alphas are pinned (refinement) */
+                                   lanes per pixel where the alphas are pinned (refinement); 6 as 3 (first pass)
+                                   and 5 (refinement) with the bookkeeping rolled over the layers; 7 the
+                                   refinement of 6 with its start and bounds in global memory, 4 blocks per SM
+                                   (first passes run 3). Default: 3 for the first pass, 7 for the refinement.
+                                   Every variant gives the same results. */
     int32_t fp32_outer;         /* FP32 precision with resolve_misses: outer steps of the FP32 solve before a
                                    pixel is left to the FP64 re-solve (default 9; 0 = outer);
                                    a pixel stopped there unconverged is always re-solved */

@@ -388,7 +388,7 @@ def test_fp64_kernel_variants_are_bit_identical(cuda, case):
     else:
         wl, opaque, smooth = syn.generate(64, 48, [0, 1, 2], (4.0, 12.0), seed=7, comp=syn.PLUS), False, False
     runs = {}
-    for v1, v2 in ((0, 2), (2, 5), (3, 5), (6, 6)):
+    for v1, v2 in ((0, 2), (2, 5), (3, 5), (6, 6), (7, 7)):
         first, st1, c1, _ = cuda.unmix_ex(wl.image, wl.layers, opaque=opaque, with_counters=True,
                                           solver=solver(cuda, 1, radius=3, fp64_variant=v1))
         final, st2, c2, _ = cuda.refine_ex(wl.image, first, wl.layers, opaque=opaque, smooth=smooth,

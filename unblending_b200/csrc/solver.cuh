@@ -92,7 +92,8 @@ enum : int { kRolled = 8 };
 enum : int { kTriple = 16 };
 // kColdGlobal (with global history): the cold values (best point, outer-step
 // start, start-0 seed) follow the history in the lane's global array, which
-// shrinks the shared-memory slice.
+// shrinks the shared-memory slice; with kBookRolled and three lanes, so does
+// the pinned alphas' gradient at x.
 enum : int { kColdGlobal = 32 };
 // kBookRolled (with kVectorsShared, kRolled and the global history): the
 // trial point and the trial gradient live only in the lane's slice (the
@@ -268,7 +269,8 @@ template <class T, int L, int S> struct LaneSlice {
     static constexpr int kScratch = history_of(S) == kHistRegisters ? kHist : kCoeff + 2 * kHistory;
     // kBookRolled with three lanes: the pinned alphas' gradient at x.
     static constexpr int kGa3 = kScratch + (kRolledEval ? 5 * L : 0);
-    static constexpr int kValues = kGa3 + (((S & kBookRolled) && (S & kTriple)) ? L : 0);
+    // (with kColdGlobal that slot follows the cold values in the global array)
+    static constexpr int kValues = kGa3 + (((S & kBookRolled) && (S & kTriple) && !(S & kColdGlobal)) ? L : 0);
     __device__ __forceinline__ static T& value(int k) {
         return reinterpret_cast<T*>(solver_smem)[k * kSliceStride + threadIdx.x];
     }
@@ -393,7 +395,9 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if constexpr (BR) return Slice::value(Slice::kScratch + L + l); else return na3_[l];
     }
     __device__ __forceinline__ T& GA3(int l) const {
-        if constexpr (BR) return Slice::value(Slice::kGa3 + l); else return ga3_[l];
+        if constexpr (BR && (S & kColdGlobal) != 0) return hist.base[size_t(2 * kHistory * L + 3 * L + l) * hist.lanes];
+        else if constexpr (BR) return Slice::value(Slice::kGa3 + l);
+        else return ga3_[l];
     }
     __device__ __forceinline__ T& best(int l) const { return cold(l); }
     __device__ __forceinline__ T& ox(int l) const { return cold(L + l); }

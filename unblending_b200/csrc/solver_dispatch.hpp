@@ -22,8 +22,10 @@ namespace unb {
 // alphas are pinned, so no alpha lane: 10 pixels per warp), FP32 as 3 and
 // FP64 as 2 otherwise; first passes run variant 3 / 2 for it.
 // FP64 variant 6: 3 (first pass) and 5 (refinement) with the bookkeeping's
-// per-layer loops rolled, the trial point and gradient in the slice.
-constexpr int kFp32Variants = 6, kFp64Variants = 7;
+// per-layer loops rolled, the trial point and gradient in the slice. FP64
+// variant 7: the refinement of 6 with its cold values in the global array,
+// capped for 4 blocks per SM (first passes run 3).
+constexpr int kFp32Variants = 6, kFp64Variants = 8;
 inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant == 4; }
 // Blocks per SM that a global-history array is sized for (the launch clamps
 // its grid to the array).

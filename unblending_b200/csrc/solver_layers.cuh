@@ -66,6 +66,11 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
             return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal | kBookRolled, 4, BATCH>(
                 m, c, a, threads, sms, s);
         else return cudaErrorInvalidValue;
+    case 7:   // 6 with the refinement's cold values in the global array, 4 blocks per SM; first passes run 3
+        if constexpr (R && !BATCH)
+            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple | kBookRolled | kColdGlobal, 4, BATCH>(
+                m, c, a, threads, sms, s);
+        else return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;
     }
 }

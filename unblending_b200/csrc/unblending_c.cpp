@@ -256,8 +256,10 @@ int default_fp32_variant(int L, bool refine) { (void)L; return refine ? 5 : 3; }
 // smaller instruction footprint cut instruction-fetch stalls from 3.6 to 1.4
 // cycles per issue): 106.5 -> 102.5 ms. The first pass keeps variant 3 (its
 // rolled form ran 145 against 139 ms: more instructions, and loads of its
-// global cold values no longer issued together).
-int default_fp64_variant(bool refine) { return refine ? 6 : 3; }
+// global cold values no longer issued together). The refinement of 6 with its
+// cold values in the global array too (variant 7, 4 blocks per SM instead of
+// 3): 94.7 -> 94.0 ms with the colour-ordered queue.
+int default_fp64_variant(bool refine) { return refine ? 7 : 3; }
 int fp64_variant(const unblending_solver_options& so, bool refine) {
     return so.fp64_variant >= 0 ? so.fp64_variant : default_fp64_variant(refine);
 }
@@ -265,8 +267,9 @@ int fp64_variant(const unblending_solver_options& so, bool refine) {
 // Bytes of a global-memory L-BFGS history array for L layers and values of
 // `elem` bytes, sized for kGlobalHistoryBlocksPerSm blocks on every SM.
 size_t history_lanes(int sms) { return size_t(kGlobalHistoryBlocksPerSm) * sms * kSliceStride; }
-// (the history, then the cold values of the variants that keep them there).
-size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * (2 * kHistory + 3) * L * elem; }
+// (the history, then the cold values of the variants that keep them there,
+// then the three-lane refinement's pinned-alpha gradient at x).
+size_t history_bytes(int L, size_t elem, int sms) { return history_lanes(sms) * (2 * kHistory + 4) * L * elem; }
 
 // Points `a` at a history array when the kernel variant keeps its history in
 // global memory.
