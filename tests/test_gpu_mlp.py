@@ -5,7 +5,7 @@ import pytest
 
 import oracle
 from tests import mlp_reference as ref
-from tests.parity import report
+from tests.parity import PIXEL_FRACTION, report
 from tests.test_mlp_reference import random_model
 from unblending_b200 import synthetic as syn
 
@@ -65,5 +65,12 @@ def test_trained_warm_start_reduces_solver_work(cuda):
     # The learned start saves objective evaluations and stays feasible.
     assert wc[:, 0].mean() < cc[:, 0].mean()
     assert wstats["failed"] <= cstats["failed"] + 0.01 * test.pixels
-    # Final objective no worse than the cold start's on most pixels.
-    assert rw["frac_objective"] >= 0.5
+    # It cannot meet the parity bar: the reference's result is where its own
+    # trajectory stops at a loose tolerance, and another start stops
+    # elsewhere. What it must do is solve the same problem at least as well:
+    # an objective no worse than the reference's on most pixels and lower on
+    # average (measured: 70 % of pixels, mean -0.14 on this image; the cold
+    # start matches the reference to 1e-13), with no more pixels left unsolved.
+    assert rw["frac_objective"] >= 0.6
+    assert rw["mean_objective_delta"] < 0.0
+    assert rc["frac_rgba_1e-3"] >= PIXEL_FRACTION and rc["frac_objective"] >= PIXEL_FRACTION
