@@ -118,7 +118,7 @@ def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> O
 def solver_options(precision=PRECISION_FP64, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
                    outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0,
                    kernel_variant=-1, warm_start=None, fp64_variant=-1, fp32_outer=9,
-                   gradient_quorum=3, frozen_stop=4, pixel_order=1) -> SolverOptions:
+                   gradient_quorum=4, frozen_stop=4, pixel_order=1) -> SolverOptions:
     """unblending_solver_options with UNBLENDING_SOLVER_OPTIONS_INIT's defaults."""
     so = SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
                        outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant,

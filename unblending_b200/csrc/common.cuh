@@ -61,7 +61,7 @@ struct SolverControls {
     int inner = 256, outer = 22, starts = 1;
     double inner_tolerance = 5e-3, outer_tolerance = 5e-3;
     int gradient_on_first_trial = 1;   // fuse the first line-search trial's gradient
-    int gradient_quorum = 3;           // eighths of a warp's live pixels that start a gradient evaluation
+    int gradient_quorum = 4;           // eighths of a warp's live pixels that start a gradient evaluation
     int direction_quorum = 0;          // eighths of a warp's live pixels that start a new direction (0 = no wait)
     int cap_is_miss = 0;               // a pixel that reaches the outer cap unconverged is a miss
     int frozen_stop = 0;               // stop after this many outer steps that move neither x nor the best point
