@@ -339,6 +339,27 @@ def test_colour_ordered_queue_leaves_results_unchanged(cuda, precision):
     assert np.array_equal(bands[0].reshape(outs[0][0].shape), outs[0][0])
 
 
+def test_colour_order_of_values_outside_the_unit_cube(cuda):
+    """The queue order quantizes each pixel's target colour: values below 0
+    (and NaN) fall in the lowest level, values of 1 and above in the highest.
+    Images holding such values are solved to the same outputs and statuses in
+    either order (NaN outputs compared as equal)."""
+    wl = syn.workload("rgb1024_l5", 40, 24)
+    image = wl.image.copy()
+    flat = image.reshape(-1, 3)
+    flat[3] = (-0.5, 0.2, 1.7)
+    flat[10] = (float("nan"), 0.5, 0.5)
+    flat[17] = (1.0, 1.0, float("inf"))
+    flat[30] = (0.0, -1e300, 2.0)
+    outs = []
+    for order in (1, 0):
+        so = solver(cuda, 1, pixel_order=order)
+        out, status, _, _ = cuda.unmix_ex(image, wl.layers, solver=so)
+        outs.append((out, status))
+    assert np.array_equal(outs[0][0], outs[1][0], equal_nan=True)
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
 FROZEN_CASES = [
     ("rgb1024_l5", 160, 128, None),
     ("rgb4096_l6", 160, 128, None),
