@@ -286,7 +286,19 @@ def reference_decomposition(wl, threads):
     t2 = time.perf_counter()
     final = reference_refine(impl, wl, first, targets, idx, threads)
     t3 = time.perf_counter()
-    return first, final, {"unmix_s": t1 - t0, "filter_s": t2 - t1, "refine_s": t3 - t2, "total_s": t3 - t0}, kind
+    times = {"unmix_s": t1 - t0, "filter_s": t2 - t1, "refine_s": t3 - t2, "total_s": t3 - t0}
+    # One core: both solves of a seeded sample of the image's pixels (the
+    # filter's share of the all-core time is small and is left out here).
+    sample = np.sort(np.random.default_rng(17).choice(n, size=min(n, 4096), replace=False))
+    s0 = time.perf_counter()
+    reference_unmix(impl, wl, sample, 1)
+    s1 = time.perf_counter()
+    reference_refine(impl, wl, first, targets[:, sample], sample, 1)
+    s2 = time.perf_counter()
+    times["single_core"] = {"value": len(sample) / (s2 - s0), "unit": UNIT, "cores": 1,
+                            "sample": f"both solves of {len(sample)} seeded pixels of the image, one thread",
+                            "unmix_s": s1 - s0, "refine_s": s2 - s1}
+    return first, final, times, kind
 
 
 def parity_whole(wl, first_gpu, final_gpu, ref_first, ref_final, threads, sample_seed=0):
