@@ -531,6 +531,55 @@ def config_leg(U, torch, name, stream, flush, steps, warmup, threads, whole_pari
     return out
 
 
+def batch_leg(U, torch, stream, flush, threads):
+    """The BASELINE's uneven batch (64 images, sides 256-2048, 3-6 layers)
+    through the batched first pass with the default solve: one warm-up call
+    (which also builds and captures the plan), one timed replay, and the
+    parity of 8,192 seeded pixels spread over the images against the
+    reference's FP64 solver."""
+    import oracle
+    from tests.parity import report
+    wls = batch_workload()
+    n = sum(w.pixels for w in wls)
+    imgs = [torch.from_numpy(w.image.reshape(-1)).cuda() for w in wls]
+    outs = [torch.empty(4 * len(w.layers) * w.pixels, dtype=torch.float64, device="cuda") for w in wls]
+    jobs = [dict(width=w.width, height=w.height, d_image=i.data_ptr(), layers=w.layers, d_output=o.data_ptr())
+            for w, i, o in zip(wls, imgs, outs)]
+    so = U.solver_options()
+    st = U.unmix_batch_device(jobs, solver=so, stream=stream, stats=True)
+    torch.cuda.synchronize()
+    flush.fill_(1.0)
+    ext = torch.cuda.ExternalStream(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    U.unmix_batch_device(jobs, solver=so, stream=stream)
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"workload": batch_label(wls), "value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": 1,
+           "warmup": 1, "gpu_launches": U.last_launch_count(), "failed": st["failed"]}
+    if threads:
+        impl, kind = reference_impl()
+        rng = np.random.default_rng(23)
+        totals, rows = {}, []
+        for w, o in zip(wls, outs):
+            L = len(w.layers)
+            k = max(1, int(round(8192 * w.pixels / n)))
+            idx = np.sort(rng.choice(w.pixels, size=min(k, w.pixels), replace=False))
+            rx = reference_unmix(impl, w, idx, threads)
+            gx = oracle.unpack(o.cpu().numpy().reshape(L, w.height, w.width, 4), L)[idx]
+            r = report(oracle.pack(gx, L, len(idx), 1), oracle.pack(rx, L, len(idx), 1), w.layers, False)
+            rows.append((len(idx), r))
+        m = sum(c for c, _ in rows)
+        for key in ("frac_rgba_1e-3", "frac_objective"):
+            totals[key] = sum(c * r[key] for c, r in rows) / m
+        totals["max_rgba"] = max(r["max_rgba"] for _, r in rows)
+        out["parity"] = {"sample": f"{m} seeded pixels over the {len(wls)} images", "kind": kind, **totals}
+    del imgs, outs
+    torch.cuda.empty_cache()
+    return out
+
+
 def b200_arm(args):
     import torch
     from unblending_b200 import dist
@@ -691,6 +740,7 @@ def b200_arm(args):
             "rgb256_l3": config_leg(U, torch, "rgb256_l3", stream.cuda_stream, flush, args.steps, args.warmup,
                                     threads, True),
             "rgb4096_l6": config_leg(U, torch, "rgb4096_l6", stream.cuda_stream, flush, 1, 1, threads, False),
+            "batch64": batch_leg(U, torch, stream.cuda_stream, flush, threads),
         }
     if rank == 0:
         print(json.dumps(line), flush=True)
