@@ -17,6 +17,8 @@
 #include <stdexcept>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/unblending.h"
 #include "../../include/unblending_b200.h"
 #include "solver_dispatch.hpp"
@@ -40,6 +42,16 @@ void ck(cudaError_t e) {
 }
 
 thread_local int64_t t_launches = 0;
+
+// NVTX range over a host-side scope (a public call, or the enqueueing of one
+// stage of a pass), seen by Nsight tools; without a tool attached it costs a
+// null check.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 // Grow-only device allocation.
 struct Buffer {
@@ -439,6 +451,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         fstatus = c.fstatus.get<int32_t>(n);
         f.targets = targets; f.status = fstatus;
         f.scratch = R.radius > 0 ? c.scratch.get<double>(filter_scratch_doubles(sp.width, sp.height, L, sp.smooth)) : nullptr;
+        const Range range("guided filter");
         ck(launch_filter(f, s));
         t_launches += filter_launches(sp.width, R.radius);
     }
@@ -461,6 +474,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         const int count = io.pixel_count >= 0 ? io.pixel_count : int(n);
         int32_t* order = c.order.get<int32_t>(size_t(count));
         uint32_t* cells = c.order_cells.get<uint32_t>(order_cells(count));
+        const Range range("queue order");
         ck(launch_pixel_order(io.image, io.first_pixel, count, cells, order, c.sms, s));
         t_launches += 4;
         a.order = order;
@@ -479,6 +493,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     void* history = c.history.get<unsigned char>(history_bytes(L, sizeof(double), c.sms));
     if (so.precision == UNBLENDING_PRECISION_FP64) {
         attach_history(a, history, true, fp64_variant(so, refine), c.sms);
+        const Range range(refine ? "refinement solve (fp64)" : "first-pass solve (fp64)");
         ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads,
                              c.sms, s));
         ++t_launches;
@@ -502,6 +517,7 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
         const int variant = so.kernel_variant >= 0 ? so.kernel_variant : default_fp32_variant(L, refine);
         attach_history(a, history, false, variant, c.sms);
         a.tally = R.tally + 2;
+        const Range range(refine ? "refinement solve (fp32 + fp64 re-solve)" : "first-pass solve (fp32 + fp64 re-solve)");
         ck(launch_solve_fp32(L, refine, variant, make_models<float>(layers, L), ctl32, a, threads, c.sms, s));
         ++t_launches;
         ck(cudaEventRecord(c.ev[2], s));
@@ -584,6 +600,7 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
                   const unblending_solver_options* solver, double* output, size_t output_capacity, int32_t* status,
                   uint32_t* counters, unblending_stats* stats, bool refine) {
     t_launches = 0;
+    const Range range(refine ? "unblending_refine" : "unblending_unmix");
     Spec sp;
     int32_t rc = validate(image, layers, layer_count, options, output, output_capacity, refine, first, first_size, sp,
                           false);
@@ -658,6 +675,7 @@ int32_t device_call(int32_t width, int32_t height, const double* image, const un
                     int32_t row_end = -1) {
     t_launches = 0;
     unblending_rgb_view view{image, 0, width, height, 0};
+    const Range range(refine ? "unblending_refine_device" : "unblending_unmix_device");
     Spec sp;
     int32_t rc = validate(&view, layers, layer_count, options, output, 0, refine, first, 0, sp, true);
     if (rc != UNBLENDING_OK) return rc;
@@ -788,6 +806,7 @@ int64_t unblending_last_launch_count(void) { return t_launches; }
 int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t count, const unblending_options* options,
                                       const unblending_solver_options* solver, void* stream, unblending_stats* stats) {
     t_launches = 0;
+    const Range range("unblending_unmix_batch_device");
     if (!jobs || count < 1) return UNBLENDING_INVALID_ARGUMENT;
     if (stats && stats->struct_size < sizeof(unblending_stats)) return UNBLENDING_INVALID_ARGUMENT;
     unblending_solver_options so;
