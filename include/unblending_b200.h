@@ -76,11 +76,16 @@ typedef struct unblending_solver_options {
                                    together take similar paths through the method; 0 image order. Results do not
                                    depend on it. A caller built against the previous layout, whose struct_size
                                    ends before this field, gets the default. */
+    int32_t defer_outer;        /* FP64 refinement solve (kernel variant 7, the default): a pixel still unsolved
+                                   when it reaches this outer step leaves the solve launch with its state and is
+                                   resumed, with the other such pixels, by a second launch right behind it; the
+                                   pixels the method struggles with then share warps. 0 = no deferral. Results do
+                                   not depend on it. Default 8 */
 } unblending_solver_options;
 
 #define UNBLENDING_SOLVER_OPTIONS_INIT \
     { (uint32_t)sizeof(unblending_solver_options), UNBLENDING_PRECISION_FP64, 1, -1, 1e-4, 1, 256, 22, 5e-3, 5e-3, 0, -1, \
-      NULL, -1, 9, 4, 4, 1 }
+      NULL, -1, 9, 4, 4, 1, 8 }
 
 /* Learned warm start (no counterpart in the reference). A per-pixel MLP,
  * 30 inputs (RGB of the clamped 3x3 neighbourhood, and log(1/256 + c) of the

@@ -128,7 +128,8 @@ def test_solver_option_validation(small):
     for bad in [dict(precision=3), dict(starts=0), dict(starts=4), dict(epsilon=0.0), dict(inner=0),
                 dict(threads_per_block=48), dict(resolve_misses=2), dict(fp32_outer=-1), dict(gradient_quorum=9),
                 dict(gradient_quorum=-1), dict(frozen_stop=-1), dict(kernel_variant=6),
-                dict(fp64_variant=8), dict(pixel_order=2), dict(pixel_order=-1)]:
+                dict(fp64_variant=8), dict(pixel_order=2), dict(pixel_order=-1),
+                dict(defer_outer=-1)]:
         so = U.solver_options(**bad)
         with pytest.raises(ValueError):
             U.unmix_ex(small.image, small.layers, solver=so)

@@ -360,6 +360,41 @@ def test_colour_order_of_values_outside_the_unit_cube(cuda):
     assert np.array_equal(outs[0][1], outs[1][1])
 
 
+@pytest.mark.parametrize("case", range(3))
+def test_deferred_pixels_leave_results_unchanged(cuda, case):
+    """The FP64 refinement defers the pixels still unsolved at outer step
+    defer_outer to a second launch that resumes them from their saved state:
+    outputs, statuses and work counters equal those of the undeferred solve,
+    also when the slots run out (defer_outer 1 defers most pixels, past the
+    slots for a quarter of them), with three starts, and for row ranges."""
+    import torch
+    starts = 3 if case == 1 else 1
+    wl = syn.workload("rgb1024_l5", 96, 80) if case < 2 else syn.generate(64, 48, [0, 6, 7, 9, 1], (8.0, 40.0), seed=8)
+    first, _, _, _ = cuda.unmix_ex(wl.image, wl.layers, solver=solver(cuda, 1, starts=starts))
+    runs = {}
+    for defer in (0, 8, 3, 1):
+        so = solver(cuda, 1, radius=3, starts=starts, defer_outer=defer)
+        runs[defer] = cuda.refine_ex(wl.image, first, wl.layers, smooth=True, solver=so, with_counters=True)[:3]
+    for defer in (8, 3, 1):
+        for a, b in zip(runs[0], runs[defer]):
+            assert np.array_equal(a, b), defer
+    if case == 2:
+        n, L = wl.pixels, len(wl.layers)
+        d_img = torch.from_numpy(wl.image.reshape(-1)).cuda()
+        d_first = torch.from_numpy(first.reshape(-1)).cuda()
+        bands = []
+        for defer in (0, 1):
+            so = solver(cuda, 1, radius=3, defer_outer=defer)
+            d_out = torch.full((4 * L * n,), float("nan"), dtype=torch.float64, device="cuda")
+            for r0, r1 in ((0, 17), (17, 48)):
+                cuda.refine_device_rows(wl.width, wl.height, d_img.data_ptr(), wl.layers, d_first.data_ptr(),
+                                        d_out.data_ptr(), r0, r1, smooth=True, solver=so)
+            torch.cuda.synchronize()
+            bands.append(d_out.cpu().numpy())
+        assert np.array_equal(bands[0], bands[1])
+        assert np.array_equal(bands[0].reshape(runs[0][0].shape), runs[0][0])
+
+
 FROZEN_CASES = [
     ("rgb1024_l5", 160, 128, None),
     ("rgb4096_l6", 160, 128, None),

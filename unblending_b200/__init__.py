@@ -60,7 +60,7 @@ class SolverOptions(ctypes.Structure):
                 ("outer_tolerance", ctypes.c_double), ("threads_per_block", ctypes.c_int32),
                 ("kernel_variant", ctypes.c_int32), ("warm_start", ctypes.c_void_p), ("fp64_variant", ctypes.c_int32),
                 ("fp32_outer", ctypes.c_int32), ("gradient_quorum", ctypes.c_int32),
-                ("frozen_stop", ctypes.c_int32), ("pixel_order", ctypes.c_int32)]
+                ("frozen_stop", ctypes.c_int32), ("pixel_order", ctypes.c_int32), ("defer_outer", ctypes.c_int32)]
 
 
 class Mlp(ctypes.Structure):
@@ -118,12 +118,12 @@ def options(opaque=True, smooth=False, backend=BACKEND_AUTO, concurrency=0) -> O
 def solver_options(precision=PRECISION_FP64, starts=1, radius=-1, epsilon=1e-4, resolve_misses=True, inner=256,
                    outer=22, inner_tolerance=5e-3, outer_tolerance=5e-3, threads_per_block=0,
                    kernel_variant=-1, warm_start=None, fp64_variant=-1, fp32_outer=9,
-                   gradient_quorum=4, frozen_stop=4, pixel_order=1) -> SolverOptions:
+                   gradient_quorum=4, frozen_stop=4, pixel_order=1, defer_outer=8) -> SolverOptions:
     """unblending_solver_options with UNBLENDING_SOLVER_OPTIONS_INIT's defaults."""
     so = SolverOptions(ctypes.sizeof(SolverOptions), precision, starts, radius, epsilon, int(resolve_misses), inner,
                        outer, inner_tolerance, outer_tolerance, threads_per_block, kernel_variant,
                        ctypes.addressof(warm_start) if warm_start is not None else None, fp64_variant, fp32_outer,
-                       gradient_quorum, frozen_stop, pixel_order)
+                       gradient_quorum, frozen_stop, pixel_order, defer_outer)
     so._keep = warm_start   # the model must outlive the options
     return so
 

@@ -67,6 +67,11 @@ struct SolverControls {
     int frozen_stop = 0;               // stop after this many outer steps that move neither x nor the best point
 };
 
+// Words a lane of a deferred pixel keeps (SolveArgs::defer_state): x, the
+// best point and the start seed (L each), up to L multipliers, and seven
+// scalars.
+__host__ __device__ constexpr int defer_words(int L) { return 4 * L + 7; }
+
 // One image of a batched first pass: its pixels occupy global queue indices
 // [offset, offset + n) of its layer-count group.
 struct BatchJob {
@@ -120,6 +125,21 @@ struct SolveArgs {
     // Without a list: optional queue order, the pixel index of each queue
     // index (a permutation of the pixels the launch solves); null = in order.
     const int32_t* order = nullptr;
+    // With a list: at most list_limit of its entries are solved.
+    int list_limit = 0x7fffffff;
+    // Deferral (defer_outer > 0): a pixel about to begin outer step
+    // defer_outer (counted from 0) leaves the launch with its state at that
+    // point in slot k of defer_state (k from *defer_count, up to
+    // defer_capacity slots; past that it carries on) and its queue index in
+    // defer_list[k]. A launch with resume set and list = defer_list resumes
+    // entry k of its list from slot k at that outer step. defer_state holds
+    // values of the solve's type: word w of lane q of slot k at
+    // [w * defer_capacity * 4 + k * 4 + q], defer_words(L) words a lane.
+    int defer_outer = 0, defer_capacity = 0;
+    int32_t* defer_list = nullptr;
+    int32_t* defer_count = nullptr;
+    void* defer_state = nullptr;
+    int resume = 0;
 };
 
 }  // namespace unb

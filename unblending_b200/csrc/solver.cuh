@@ -286,7 +286,12 @@ enum : int { aEval = 0, aBeginIter, aNextTrial, aAccept, aEndOuter, aBeginStart,
 
 // BATCH: pixels of many images (one layer-count group); the quad's layer
 // models are those of its current image in the device model table.
-template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSolver {
+// MODE: kPlain; kDefers, a launch that defers pixels (SolveArgs::defer_*);
+// kResumes, the launch that resumes them. Only the code a mode runs is
+// compiled into its kernel.
+enum : int { kPlain = 0, kDefers = 1, kResumes = 2 };
+
+template <class T, int L, bool REFINE, int S, bool BATCH = false, int MODE = kPlain> struct QuadSolver {
     // Residual rows of a lane: the alpha lane of a refinement owns the L rows
     // of the pinned alphas; a colour lane owns one (three-lane groups have
     // colour lanes only). RA: the pinned alphas a lane keeps.
@@ -999,6 +1004,8 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         if (!(motion < tol2 && feasible)) {
             if (outer + 1 < ctl.outer) {
                 ++outer;
+                if constexpr (MODE == kDefers)
+                    if (outer == a.defer_outer && defer()) return aFetch;
                 return aBeginOuter;
             }
             // A shortened FP32 solve (the FP64 re-solve behind it) hands an
@@ -1153,6 +1160,62 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         return aAccept;
     }
 
+    // ------------------------------------------------------- deferral --
+    // The state a pixel needs to begin an outer step (SolveArgs::defer_*):
+    // x, the best point, the start-0 seed, the multipliers, rho, the best
+    // point's norm and energy, and the outer-step, frozen-step and start
+    // counters. Everything else is set again by the outer step's first
+    // evaluation. Word w of this lane in slot k: [w * capacity * 4 + k * 4 + q].
+    __device__ bool defer() {
+        static_assert(3 * L + R + 7 <= defer_words(L), "the deferred state fits its slot");
+        int slot = 0;
+        if (Q.q == 0) slot = int(atomicAdd(a.defer_count, 1));
+        slot = Q.from(slot, 0);
+        if (slot >= a.defer_capacity) return false;
+        if (Q.q == 0) a.defer_list[slot] = int32_t(gidx);
+        T* st = static_cast<T*>(a.defer_state) + size_t(slot) * 4 + Q.q;
+        const size_t w = size_t(a.defer_capacity) * 4;
+        int k = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) st[size_t(k++) * w] = X(l);
+#pragma unroll
+        for (int l = 0; l < L; ++l) st[size_t(k++) * w] = best(l);
+#pragma unroll
+        for (int l = 0; l < L; ++l) st[size_t(k++) * w] = init(l);
+#pragma unroll
+        for (int r = 0; r < R; ++r) st[size_t(k++) * w] = lam[r];
+        st[size_t(k++) * w] = rho;
+        st[size_t(k++) * w] = best_norm;
+        st[size_t(k++) * w] = best_energy;
+        st[size_t(k++) * w] = T(outer);
+        st[size_t(k++) * w] = T(frozen);
+        st[size_t(k++) * w] = T(start);
+        st[size_t(k++) * w] = have_best ? T(1) : T(0);
+        return true;
+    }
+
+    __device__ void restore(int slot) {
+        const T* st = static_cast<const T*>(a.defer_state) + size_t(slot) * 4 + Q.q;
+        const size_t w = size_t(a.defer_capacity) * 4;
+        int k = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) X(l) = st[size_t(k++) * w];
+#pragma unroll
+        for (int l = 0; l < L; ++l) best(l) = st[size_t(k++) * w];
+#pragma unroll
+        for (int l = 0; l < L; ++l) init(l) = st[size_t(k++) * w];
+#pragma unroll
+        for (int r = 0; r < R; ++r) lam[r] = st[size_t(k++) * w];
+        rho = st[size_t(k++) * w];
+        best_norm = st[size_t(k++) * w];
+        best_energy = st[size_t(k++) * w];
+        outer = int(st[size_t(k++) * w]);
+        frozen = int(st[size_t(k++) * w]);
+        start = int(st[size_t(k++) * w]);
+        have_best = st[size_t(k++) * w] != T(0);
+        capped = false;
+    }
+
     // ------------------------------------------------------------ pixels --
     // Loads pixel `i`: targets, bounds and the start-0 seed.
     __device__ __forceinline__ void load(int i) {
@@ -1188,7 +1251,7 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
         have_best = false;
         capped = false;
         best_norm = T(INFINITY); best_energy = T(INFINITY);
-        if (a.counters && Q.q == 0)
+        if (a.counters && Q.q == 0 && MODE != kResumes)
 #pragma unroll
             for (int k = 0; k < 5; ++k) counter(k) = 0;
     }
@@ -1284,13 +1347,19 @@ template <class T, int L, bool REFINE, int S, bool BATCH = false> struct QuadSol
             store(true);
             return aFetch;
         }
+        if constexpr (MODE == kResumes) {
+            // A pixel deferred by an earlier launch: its state at the start of
+            // the outer step it left at, from slot `job` of the list.
+            restore(job);
+            return aBeginOuter;
+        }
         start = 0;
         return aBeginStart;
     }
 
     // ------------------------------------------------------------- loop --
     __device__ void run() {
-        const int total = a.list ? *a.list_count : (a.pixel_count >= 0 ? a.pixel_count : a.n);
+        const int total = a.list ? min(*a.list_count, a.list_limit) : (a.pixel_count >= 0 ? a.pixel_count : a.n);
         bool live = !Q.extra;            // lanes of no group stay idle throughout
         int act = live ? aFetch : aEval;
         const int gq = ctl.gradient_quorum, bq = ctl.direction_quorum;

@@ -27,6 +27,12 @@ namespace unb {
 // capped for 4 blocks per SM (first passes run 3).
 constexpr int kFp32Variants = 6, kFp64Variants = 8;
 inline bool variant_global_history(bool fp64, int variant) { return fp64 ? variant >= 2 : variant == 4; }
+// FP64 variants whose kernels can defer and resume pixels (SolveArgs::
+// defer_outer / resume): the refinement's variant 7. (Deferral was measured
+// on the first pass too, where it cost more than it saved: 130 -> 133 ms
+// on the 1024x1024 five-layer image, against 91.5 -> 88.1 ms for the
+// refinement.)
+inline bool variant_defers(int variant, bool refine) { return refine && variant == 7; }
 // Blocks per SM that a global-history array is sized for (the launch clamps
 // its grid to the array).
 constexpr int kGlobalHistoryBlocksPerSm = 6;

@@ -15,19 +15,19 @@ template <class T, int L, int S, bool BATCH> struct SolveSmem {
 
 // S: storage policy (history place | kVectorsShared); MINB: blocks per SM
 // the register allocation must allow (launch bounds).
-template <class T, int L, bool REFINE, int S, int MINB, bool BATCH>
+template <class T, int L, bool REFINE, int S, int MINB, bool BATCH, int MODE = kPlain>
 __global__ void __launch_bounds__(128, MINB)
 solve_pixels(const __grid_constant__ Models<T> m, const __grid_constant__ SolverControls ctl,
              const __grid_constant__ SolveArgs a) {
-    QuadSolver<T, L, REFINE, S, BATCH> solver(&m, ctl, a);
+    QuadSolver<T, L, REFINE, S, BATCH, MODE> solver(&m, ctl, a);
     solver.run();
 }
 
-template <class T, int L, bool REFINE, int S, int MINB = 1, bool BATCH = false> struct SolveLauncher {
+template <class T, int L, bool REFINE, int S, int MINB = 1, bool BATCH = false, int MODE = kPlain> struct SolveLauncher {
     using Smem = SolveSmem<T, L, S, BATCH>;
 
     static cudaError_t occupancy(int threads, int* blocks_per_sm) {
-        auto k = solve_pixels<T, L, REFINE, S, MINB, BATCH>;
+        auto k = solve_pixels<T, L, REFINE, S, MINB, BATCH, MODE>;
         const size_t sm = Smem::bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
@@ -38,7 +38,7 @@ template <class T, int L, bool REFINE, int S, int MINB = 1, bool BATCH = false> 
 
     static cudaError_t launch(const Models<T>& m, const SolverControls& ctl, const SolveArgs& a, int blocks,
                               int threads, cudaStream_t stream) {
-        auto k = solve_pixels<T, L, REFINE, S, MINB, BATCH>;
+        auto k = solve_pixels<T, L, REFINE, S, MINB, BATCH, MODE>;
         const size_t sm = Smem::bytes(threads);
         if (sm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));

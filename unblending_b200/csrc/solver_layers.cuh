@@ -16,14 +16,24 @@ namespace unb {
 namespace {
 constexpr int kL = UNB_SOLVER_LAYERS;
 
-template <class T, bool R, int S, int B, bool BATCH>
+template <class T, bool R, int S, int B, bool BATCH, int MODE = kPlain>
 cudaError_t go(const Models<T>& m, const SolverControls& c, const SolveArgs& a, int threads, int sms, cudaStream_t s) {
-    using Launch = SolveLauncher<T, kL, R, S, B, BATCH>;
+    using Launch = SolveLauncher<T, kL, R, S, B, BATCH, MODE>;
     int per_sm = 0;
     cudaError_t e = Launch::occupancy(threads, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     return Launch::launch(m, c, a, per_sm * sms, threads, s);
+}
+
+// A kernel that can defer or resume pixels (SolveArgs::defer_outer / resume):
+// the default FP64 refinement variant, compiled once per mode.
+template <bool R, int S, int B>
+cudaError_t go_modes(const Models<double>& m, const SolverControls& c, const SolveArgs& a, int threads, int sms,
+                     cudaStream_t s) {
+    if (a.resume) return go<double, R, S, B, false, kResumes>(m, c, a, threads, sms, s);
+    if (a.defer_outer > 0) return go<double, R, S, B, false, kDefers>(m, c, a, threads, sms, s);
+    return go<double, R, S, B, false>(m, c, a, threads, sms, s);
 }
 
 template <bool R, bool BATCH>
@@ -68,7 +78,7 @@ cudaError_t fp64(int variant, const Models<double>& m, const SolverControls& c, 
         else return cudaErrorInvalidValue;
     case 7:   // 6 with the refinement's cold values in the global array, 4 blocks per SM; first passes run 3
         if constexpr (R && !BATCH)
-            return go<double, R, kHistGlobal | kVectorsShared | kRolled | kTriple | kBookRolled | kColdGlobal, 4, BATCH>(
+            return go_modes<R, kHistGlobal | kVectorsShared | kRolled | kTriple | kBookRolled | kColdGlobal, 4>(
                 m, c, a, threads, sms, s);
         else return go<double, R, kHistGlobal | kVectorsShared | kRolled | kColdGlobal, 4, BATCH>(m, c, a, threads, sms, s);
     default: return cudaErrorInvalidValue;

@@ -103,6 +103,7 @@ struct Context {
     std::mutex mutex;
     Buffer image, first, out, targets, fstatus, scratch, list_a, list_b, small, status, counters, history;
     Buffer order, order_cells;               // work-queue order of a pass (order.cu) and its counting-sort cells
+    Buffer defer_list, defer_state;          // pixels deferred by an FP64 solve launch and their state
     Buffer warm, mlp_w, mlp_b;               // warm-start network on the device
     std::vector<float> mlp_uploaded;         // parameters currently in mlp_w / mlp_b
     // Concurrent branches of a batched pass (one per layer-count group) and
@@ -240,7 +241,8 @@ int32_t resolve_solver(const unblending_solver_options* in, unblending_solver_op
                                         out.threads_per_block > 128)) ||
         out.kernel_variant < -1 || out.kernel_variant >= kFp32Variants || out.fp64_variant < -1 ||
         out.fp64_variant >= kFp64Variants || out.fp32_outer < 0 || out.gradient_quorum < 0 ||
-        out.gradient_quorum > 8 || out.frozen_stop < 0 || (out.pixel_order != 0 && out.pixel_order != 1))
+        out.gradient_quorum > 8 || out.frozen_stop < 0 || (out.pixel_order != 0 && out.pixel_order != 1) ||
+        out.defer_outer < 0)
         return UNBLENDING_INVALID_ARGUMENT;
     return UNBLENDING_OK;
 }
@@ -494,9 +496,34 @@ PassResult enqueue_pass(Context& c, const Spec& sp, bool refine, const unblendin
     if (so.precision == UNBLENDING_PRECISION_FP64) {
         attach_history(a, history, true, fp64_variant(so, refine), c.sms);
         const Range range(refine ? "refinement solve (fp64)" : "first-pass solve (fp64)");
+        const int solved = io.pixel_count >= 0 ? io.pixel_count : int(n);
+        if (so.defer_outer > 0 && solved > 0 && variant_defers(fp64_variant(so, refine), refine)) {
+            // Pixels still unsolved at outer step defer_outer leave this
+            // launch (up to a quarter of its pixels; the rest carry on) ...
+            a.defer_outer = so.defer_outer;
+            a.defer_capacity = std::max(1, solved / 4);
+            a.defer_list = c.defer_list.get<int32_t>(size_t(a.defer_capacity));
+            a.defer_count = reinterpret_cast<int32_t*>(queues + 3);
+            a.defer_state = c.defer_state.get<double>(size_t(a.defer_capacity) * 4 * size_t(defer_words(L)));
+        }
         ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, a, threads,
                              c.sms, s));
         ++t_launches;
+        if (a.defer_outer > 0) {
+            // ... and are resumed together by the next launch (queue 2), from
+            // the state they left with: each pixel takes the same steps.
+            SolveArgs d = a;
+            d.defer_outer = 0;
+            d.resume = 1;
+            d.list = a.defer_list; d.list_count = a.defer_count; d.list_limit = a.defer_capacity;
+            d.order = nullptr;
+            d.queue = queues + 2;
+            d.input_status = nullptr; d.input_failed = nullptr;
+            ck(launch_solve_fp64(L, refine, fp64_variant(so, refine), make_models<double>(layers, L), ctl, d, threads,
+                                 c.sms, s));
+            ++t_launches;
+            a.defer_outer = 0;
+        }
         ck(cudaEventRecord(c.ev[2], s));
         if (a.warm) {
             // Pixels that the learned start leaves unsolved get the plain
@@ -843,6 +870,7 @@ int32_t unblending_unmix_batch_device(const unblending_image_job* jobs, int32_t 
     put(&so.gradient_quorum, sizeof(so.gradient_quorum));
     put(&so.frozen_stop, sizeof(so.frozen_stop));
     put(&so.pixel_order, sizeof(so.pixel_order));
+    put(&so.defer_outer, sizeof(so.defer_outer));
     for (int k = 0; k < count; ++k) {
         const auto& J = jobs[k];
         put(&J.width, sizeof(J.width)); put(&J.height, sizeof(J.height));
