@@ -15,8 +15,10 @@
 // passes (rows, then columns), O(1) per pixel for any radius, as the
 // reference's GPU filter is (row prefix scans, guided_filter.cuh:49-66):
 //   * rows: one CTA per image row; each plane of the row is prefix-summed
-//     across the CTA in shared memory (FP64) and the window sums are prefix
-//     differences, read and written with coalesced accesses. The first box's
+//     across the CTA in shared memory (FP64; padding keeps the threads'
+//     chunk scans free of bank conflicts) and the
+//     window sums are prefix differences, read and written with coalesced
+//     accesses. The first box's
 //     planes (I, I I^T, p, I p) are formed from the image and the first pass
 //     inside this kernel instead of being packed to memory first.
 //   * columns: one thread per (plane, column, segment of rows) with a
@@ -30,10 +32,32 @@ namespace {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-constexpr int kRowThreads = 256;
-// Widest row the prefix pass keeps in shared memory (96 KiB of doubles);
-// wider images take the one-thread-per-row sliding pass.
+// Threads of a row-pass CTA: 128 at 64 registers gives eight CTAs per SM,
+// so the rows of a 1024-high image run in one wave of 148 x 8 CTAs.
+constexpr int kRowThreads = 128;
+// Widest row the prefix pass keeps in shared memory (at most 102 KiB of
+// doubles with the padding below); wider images take the one-thread-per-row
+// sliding pass.
 constexpr int kRowPrefixMaxWidth = 12288;
+
+// Shared-memory slot of row element x in the prefix pass: thread t scans
+// elements [t*chunk, (t+1)*chunk), so the lanes of a warp are `chunk`
+// doubles apart, and an even chunk puts them in the same banks (16-way at
+// chunk 8, the 1024-wide image). One pad double after every 2^sh values,
+// 2^sh the lowest set bit of an even chunk, makes the distance between lanes
+// odd (chunk + chunk / 2^sh = m (2^sh + 1), m odd), so a warp's 32 doubles
+// fall on 16 distinct bank pairs: two wavefronts, the minimum for 8-byte
+// words. An odd chunk is conflict-free unpadded (sh = 31). Contiguous reads
+// of 32 values take at most three wavefronts.
+__host__ __device__ __forceinline__ int row_chunk(int w) { return (w + kRowThreads - 1) / kRowThreads; }
+__host__ __device__ __forceinline__ int row_pad_shift(int w) {
+    const int c = row_chunk(w);
+    if (c & 1) return 31;
+    int sh = 0;
+    while (((c >> sh) & 1) == 0) ++sh;
+    return sh;
+}
+__host__ __device__ __forceinline__ int padx(int x, int sh) { return x + (x >> sh); }
 constexpr int kColSegment = 128;   // rows per thread of the column pass
 
 // Channel value p_c of pixel i: first-pass alpha of layer c (c < L), else the
@@ -80,26 +104,27 @@ __device__ __forceinline__ double packed_value(const double* image, const double
 // the end values) / (2r+1). PACKED: plane k of the input is packed plane k,
 // formed from the image and the first pass.
 template <bool PACKED>
-__global__ void __launch_bounds__(kRowThreads)
+__global__ void __launch_bounds__(kRowThreads, 8)
 box_rows_prefix(const double* in, const double* image, const double* first, double* out, int w, int h, int planes,
                 int L, int r) {
-    extern __shared__ double sm_row[];   // w prefix values, then one total per warp
-    double* warp_total = sm_row + w;
+    extern __shared__ double sm_row[];   // w prefix values (padded), then one total per warp
+    const int sh = row_pad_shift(w);
+    double* warp_total = sm_row + padx(w - 1, sh) + 1;
     const int y = blockIdx.x;
     const size_t n = size_t(w) * h, row0 = size_t(y) * w;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    const int chunk = (w + kRowThreads - 1) / kRowThreads;
+    const int chunk = row_chunk(w);
     const int x0 = min(w, t * chunk), x1 = min(w, x0 + chunk);
     const double norm = double(2 * r + 1);
     for (int k = 0; k < planes; ++k) {
         const double* src = PACKED ? nullptr : in + size_t(k) * n + row0;
         // Coalesced load of the row into shared memory.
         for (int x = t; x < w; x += kRowThreads)
-            sm_row[x] = PACKED ? packed_value(image, first, n, L, k, row0 + x) : src[x];
+            sm_row[padx(x, sh)] = PACKED ? packed_value(image, first, n, L, k, row0 + x) : src[x];
         __syncthreads();
         // Inclusive scan: this thread's chunk, then the chunk totals.
         double s = 0.0;
-        for (int x = x0; x < x1; ++x) { s += sm_row[x]; sm_row[x] = s; }
+        for (int x = x0; x < x1; ++x) { s += sm_row[padx(x, sh)]; sm_row[padx(x, sh)] = s; }
         double incl = s;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -110,7 +135,7 @@ box_rows_prefix(const double* in, const double* image, const double* first, doub
         __syncthreads();
         double carry = incl - s;   // exclusive prefix of this thread within its warp
         for (int q = 0; q < wid; ++q) carry += warp_total[q];
-        for (int x = x0; x < x1; ++x) sm_row[x] += carry;
+        for (int x = x0; x < x1; ++x) sm_row[padx(x, sh)] += carry;
         __syncthreads();
         // Window sums: prefix differences plus the clamped copies of the end
         // values (read again from their source, exactly).
@@ -119,7 +144,7 @@ box_rows_prefix(const double* in, const double* image, const double* first, doub
         double* dst = out + size_t(k) * n + row0;
         for (int x = t; x < w; x += kRowThreads) {
             const int hi = min(x + r, w - 1), lo = x - r - 1;
-            double sum = sm_row[hi] - (lo >= 0 ? sm_row[lo] : 0.0);
+            double sum = sm_row[padx(hi, sh)] - (lo >= 0 ? sm_row[padx(lo, sh)] : 0.0);
             if (x - r < 0) sum += double(r - x) * first_v;
             if (x + r > w - 1) sum += double(x + r - (w - 1)) * last_v;
             dst[x] = sum / norm;
@@ -231,7 +256,7 @@ __global__ void finish_targets(const double* image, const double* first, const d
 cudaError_t box(const double* in, const double* image, const double* first, int L, int channels, double* tmp,
                 double* out, int w, int h, int planes, int r, cudaStream_t s) {
     if (w <= kRowPrefixMaxWidth) {
-        const size_t smem = (size_t(w) + kRowThreads / 32) * sizeof(double);
+        const size_t smem = (size_t(padx(w - 1, row_pad_shift(w))) + 1 + kRowThreads / 32) * sizeof(double);
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(image ? box_rows_prefix<true> : box_rows_prefix<false>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
