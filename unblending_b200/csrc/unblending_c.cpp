@@ -7,6 +7,7 @@
 // same validation order, same error codes, output written only on success.
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <limits>
@@ -15,6 +16,7 @@
 #include <mutex>
 #include <new>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -92,6 +94,124 @@ struct BatchPlan {
     }
 };
 
+// ------------------------------------------------------------ host copies --
+// The host-buffer entry points copy the caller's image and first pass up and
+// the results down. Page-locked host memory (cudaHostAlloc, cudaHostRegister)
+// goes to the copy engine directly. From pageable memory (a plain heap
+// buffer, as the reference's CLI passes) the driver would stage each copy
+// through small page-locked buffers of its own, one host thread at a time,
+// at a fraction of the host link's rate; such copies go instead through a
+// ring of page-locked chunks owned by the device context (Staging), each
+// chunk filled or drained by several host threads (CopyPool) while the copy
+// engine moves the previous ones.
+
+// Host threads that split one memcpy with the caller. One process-wide pool,
+// never destroyed (its threads sleep on a condition variable and end with
+// the process); concurrent calls take turns.
+class CopyPool {
+public:
+    static CopyPool& get() {
+        static CopyPool* pool = new CopyPool(helpers());
+        return *pool;
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        std::lock_guard<std::mutex> call(call_mutex_);
+        const int parts = int(threads_.size()) + 1;
+        if (parts == 1 || bytes < (size_t(1) << 20)) { std::memcpy(dst, src, bytes); return; }
+        {
+            std::lock_guard<std::mutex> l(m_);
+            job_ = Job{static_cast<char*>(dst), static_cast<const char*>(src), bytes, parts};
+            pending_ = parts - 1;
+            ++generation_;
+        }
+        wake_.notify_all();
+        run_part(job_, 0);   // the caller's share
+        std::unique_lock<std::mutex> l(m_);
+        done_.wait(l, [this] { return pending_ == 0; });
+    }
+
+private:
+    struct Job {
+        char* dst = nullptr;
+        const char* src = nullptr;
+        size_t bytes = 0;
+        int parts = 1;
+    };
+    // Helpers besides the caller: half the hardware threads, at most 7.
+    static int helpers() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        return int(std::min<unsigned>(7, hw > 2 ? hw / 2 - 1 : 0));
+    }
+    // Part k of j.parts, on 64-byte boundaries.
+    static void run_part(const Job& j, int k) {
+        const size_t per = (j.bytes / size_t(j.parts) + 63) & ~size_t(63);
+        const size_t b = std::min(j.bytes, per * size_t(k)), e = std::min(j.bytes, b + per);
+        if (e > b) std::memcpy(j.dst + b, j.src + b, e - b);
+    }
+    explicit CopyPool(int n) {
+        for (int i = 0; i < n; ++i) threads_.emplace_back([this, i] { loop(i + 1); });
+    }
+    void loop(int part) {
+        uint64_t seen = 0;
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> l(m_);
+                wake_.wait(l, [&] { return generation_ != seen; });
+                seen = generation_;
+                j = job_;
+            }
+            run_part(j, part);
+            std::lock_guard<std::mutex> l(m_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex call_mutex_, m_;
+    std::condition_variable wake_, done_;
+    Job job_;
+    int pending_ = 0;
+    uint64_t generation_ = 0;
+};
+
+// Page-locked chunks of a device context for copies of pageable buffers
+// (allocated on the first such copy), and per chunk the event of the last
+// copy that used it.
+struct Staging {
+    static constexpr size_t kChunk = size_t(8) << 20;
+    static constexpr int kSlots = 4;
+    unsigned char* ring = nullptr;
+    cudaEvent_t done[kSlots] = {};
+    Staging() = default;
+    Staging(const Staging&) = delete;
+    Staging& operator=(const Staging&) = delete;
+    ~Staging() {
+        if (ring) cudaFreeHost(ring);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
+    }
+    unsigned char* chunk(size_t k) const { return ring + (k % kSlots) * kChunk; }
+    cudaEvent_t& event(size_t k) { return done[k % kSlots]; }
+    void ensure() {
+        if (ring) return;
+        for (auto& e : done)
+            if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        void* p = nullptr;
+        ck(cudaHostAlloc(&p, kChunk * kSlots, cudaHostAllocDefault));
+        ring = static_cast<unsigned char*>(p);
+    }
+};
+
+// True for host memory the copy engine can read directly.
+bool page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
 // One per CUDA device: a stream, the solver's scratch, and timing events.
 // Calls on the same device are serialized by `mutex`.
 struct Context {
@@ -105,6 +225,7 @@ struct Context {
     Buffer order, order_cells;               // work-queue order of a pass (order.cu) and its counting-sort cells
     Buffer defer_list, defer_state;          // pixels deferred by an FP64 solve launch and their state
     Buffer warm, mlp_w, mlp_b;               // warm-start network on the device
+    Staging staging;                         // page-locked chunks for pageable caller buffers
     std::vector<float> mlp_uploaded;         // parameters currently in mlp_w / mlp_b
     // Concurrent branches of a batched pass (one per layer-count group) and
     // the events that fork them from and join them to the call's stream.
@@ -117,6 +238,51 @@ struct Context {
         for (auto& e : ev) ck(cudaEventCreate(&e));
     }
 };
+
+// Copies `bytes` of the caller's host buffer `src` to device memory `dst` on
+// stream `s`. Returns once `src` may be reused (its pageable contents are in
+// the staging chunks or on the device).
+void upload(Context& c, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes < Staging::kChunk || page_locked(src)) {
+        ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return;
+    }
+    Staging& g = c.staging;
+    g.ensure();
+    for (size_t off = 0, k = 0; off < bytes; off += Staging::kChunk, ++k) {
+        const size_t len = std::min(Staging::kChunk, bytes - off);
+        ck(cudaEventSynchronize(g.event(k)));   // the chunk's previous copy is done
+        CopyPool::get().copy(g.chunk(k), static_cast<const unsigned char*>(src) + off, len);
+        ck(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, g.chunk(k), len, cudaMemcpyHostToDevice, s));
+        ck(cudaEventRecord(g.event(k), s));
+    }
+}
+
+// Copies `bytes` of device memory `src` to the caller's host buffer `dst`
+// after the work already on stream `s`. Pageable `dst`: returns when `dst`
+// holds them. Page-locked `dst`: returns once the copy is enqueued.
+void download(Context& c, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes < Staging::kChunk || page_locked(dst)) {
+        ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        return;
+    }
+    Staging& g = c.staging;
+    g.ensure();
+    const size_t chunks = (bytes + Staging::kChunk - 1) / Staging::kChunk;
+    auto enqueue = [&](size_t k) {
+        const size_t off = k * Staging::kChunk, len = std::min(Staging::kChunk, bytes - off);
+        ck(cudaEventSynchronize(g.event(k)));   // the chunk's previous copy is done
+        ck(cudaMemcpyAsync(g.chunk(k), static_cast<const unsigned char*>(src) + off, len, cudaMemcpyDeviceToHost, s));
+        ck(cudaEventRecord(g.event(k), s));
+    };
+    for (size_t k = 0; k < std::min<size_t>(chunks, Staging::kSlots); ++k) enqueue(k);
+    for (size_t k = 0; k < chunks; ++k) {
+        const size_t off = k * Staging::kChunk, len = std::min(Staging::kChunk, bytes - off);
+        ck(cudaEventSynchronize(g.event(k)));
+        CopyPool::get().copy(static_cast<unsigned char*>(dst) + off, g.chunk(k), len);
+        if (k + Staging::kSlots < chunks) enqueue(k + Staging::kSlots);
+    }
+}
 
 Context& context() {
     static std::mutex registry_mutex;
@@ -650,14 +816,14 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
         ck(cudaEventRecord(t0, s));
         const size_t row = 3 * size_t(sp.width);
         if (sp.row_stride == row)
-            ck(cudaMemcpyAsync(d_image, image->data, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+            upload(c, d_image, image->data, 3 * n * sizeof(double), s);
         else
             ck(cudaMemcpy2DAsync(d_image, row * sizeof(double), image->data, sp.row_stride * sizeof(double),
                                  row * sizeof(double), size_t(sp.height), cudaMemcpyHostToDevice, s));
         io.image = d_image;
         if (refine) {
             double* d_first = c.first.get<double>(4 * L * n);
-            ck(cudaMemcpyAsync(d_first, first, 4 * L * n * sizeof(double), cudaMemcpyHostToDevice, s));
+            upload(c, d_first, first, 4 * L * n * sizeof(double), s);
             io.first = d_first;
         }
         io.out = c.out.get<double>(4 * L * n);
@@ -671,9 +837,9 @@ int32_t host_call(const unblending_rgb_view* image, const unblending_layer* laye
         ck(cudaStreamSynchronize(s));
         if (sp.strict && (counts[1] > 0 || counts[2] > 0)) throw SolverFailure("pixels miss the feasibility tolerance");
         ck(cudaEventRecord(c.ev[4], s));
-        ck(cudaMemcpyAsync(output, io.out, 4 * L * n * sizeof(double), cudaMemcpyDeviceToHost, s));
-        if (status) ck(cudaMemcpyAsync(status, io.status, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        if (counters) ck(cudaMemcpyAsync(counters, io.counters, 5 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        download(c, output, io.out, 4 * L * n * sizeof(double), s);
+        if (status) download(c, status, io.status, n * sizeof(int32_t), s);
+        if (counters) download(c, counters, io.counters, 5 * n * sizeof(uint32_t), s);
         ck(cudaEventRecord(t1, s));
         ck(cudaStreamSynchronize(s));
         ck(cudaGetLastError());
