@@ -192,13 +192,23 @@ struct Staging {
     }
     unsigned char* chunk(size_t k) const { return ring + (k % kSlots) * kChunk; }
     cudaEvent_t& event(size_t k) { return done[k % kSlots]; }
-    void ensure() {
-        if (ring) return;
+    // False when the chunks cannot be had (page-locked memory is a limited
+    // resource): the copy then goes to the driver directly.
+    bool ensure() {
+        if (ring) return true;
         for (auto& e : done)
-            if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                e = nullptr;
+                cudaGetLastError();
+                return false;
+            }
         void* p = nullptr;
-        ck(cudaHostAlloc(&p, kChunk * kSlots, cudaHostAllocDefault));
+        if (cudaHostAlloc(&p, kChunk * kSlots, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
         ring = static_cast<unsigned char*>(p);
+        return true;
     }
 };
 
@@ -243,12 +253,11 @@ struct Context {
 // stream `s`. Returns once `src` may be reused (its pageable contents are in
 // the staging chunks or on the device).
 void upload(Context& c, void* dst, const void* src, size_t bytes, cudaStream_t s) {
-    if (bytes < Staging::kChunk || page_locked(src)) {
+    Staging& g = c.staging;
+    if (bytes < Staging::kChunk || page_locked(src) || !g.ensure()) {
         ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
         return;
     }
-    Staging& g = c.staging;
-    g.ensure();
     for (size_t off = 0, k = 0; off < bytes; off += Staging::kChunk, ++k) {
         const size_t len = std::min(Staging::kChunk, bytes - off);
         ck(cudaEventSynchronize(g.event(k)));   // the chunk's previous copy is done
@@ -262,12 +271,11 @@ void upload(Context& c, void* dst, const void* src, size_t bytes, cudaStream_t s
 // after the work already on stream `s`. Pageable `dst`: returns when `dst`
 // holds them. Page-locked `dst`: returns once the copy is enqueued.
 void download(Context& c, void* dst, const void* src, size_t bytes, cudaStream_t s) {
-    if (bytes < Staging::kChunk || page_locked(dst)) {
+    Staging& g = c.staging;
+    if (bytes < Staging::kChunk || page_locked(dst) || !g.ensure()) {
         ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
         return;
     }
-    Staging& g = c.staging;
-    g.ensure();
     const size_t chunks = (bytes + Staging::kChunk - 1) / Staging::kChunk;
     auto enqueue = [&](size_t k) {
         const size_t off = k * Staging::kChunk, len = std::min(Staging::kChunk, bytes - off);
